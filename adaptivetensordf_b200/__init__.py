@@ -1,0 +1,66 @@
+"""B200 (sm_100a) forward-projection path of the adaptive tensorial density
+field reconstructor (HyperAcorn / adaptivetensordf).
+
+The native pieces live next to this file:
+  * libatdf_b200.so   hand-written sm_100a kernels behind the C ABI of
+                      include/atdf.h;
+  * _atdf_host*.so    the C++/libtorch host layer with the reference's
+                      operator surface (HyperTreeBase, SampleList,
+                      IndirectGridSample2D/1D, GeometryTensorQO, ...).
+Both are built in place by ``adaptivetensordf_b200.build.build()``. Importing
+this package loads them and fails loudly when they are missing: there is no
+CPU or pure-PyTorch fallback for the path.
+"""
+
+from __future__ import annotations
+
+import glob
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libatdf_b200.so")
+
+
+def _load_ext():
+    import torch  # noqa: F401  (libtorch must be loaded before the extension)
+
+    cands = glob.glob(os.path.join(_HERE, "_atdf_host*.so"))
+    if not cands or not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "adaptivetensordf_b200: native libraries are not built; run "
+            "`python -m adaptivetensordf_b200.build` (or __graft_entry__.build())"
+        )
+    from . import _atdf_host  # type: ignore
+
+    return _atdf_host
+
+
+ext = _load_ext()
+
+HyperTreeBase = ext.HyperTreeBase
+RayList = ext.RayList
+SampleList = ext.SampleList
+GeometryTensorQO = ext.GeometryTensorQO
+IndirectGridSample2D = ext.IndirectGridSample2D
+IndirectGridSample1D = ext.IndirectGridSample1D
+GradientCorrection = ext.GradientCorrection
+IntegrateSamplesXRay = ext.IntegrateSamplesXRay
+AccumulateSampleLossPerNode = ext.AccumulateSampleLossPerNode
+MseLossAndGrad = ext.MseLossAndGrad
+DecodeFeatures = ext.DecodeFeatures
+
+__all__ = [
+    "ext",
+    "LIB_PATH",
+    "HyperTreeBase",
+    "RayList",
+    "SampleList",
+    "GeometryTensorQO",
+    "IndirectGridSample2D",
+    "IndirectGridSample1D",
+    "GradientCorrection",
+    "IntegrateSamplesXRay",
+    "AccumulateSampleLossPerNode",
+    "MseLossAndGrad",
+    "DecodeFeatures",
+]

@@ -1,0 +1,298 @@
+/*
+ * atdf.h - C ABI of the B200 (sm_100a) forward-projection library
+ * (libatdf_b200.so) for the adaptive tensorial density field reconstructor.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream,
+ * launches asynchronously on that stream and returns an atdf_status. Nothing
+ * here allocates device memory: callers pass outputs and, where stated, a
+ * workspace whose size is queried first. Kernels report data-dependent
+ * problems (an index out of range, a capacity overflow) by OR-ing bits into a
+ * caller-provided device word (dev_error, see ATDF_DEVERR_*) and skipping the
+ * offending access; they never trap.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   hyperacorn/csrc/structure/HyperTree.h:463      CreateSamplesForRays
+ *   hyperacorn/csrc/structure/HyperTree.h:432      ComputeLocalSamples
+ *   hyperacorn/csrc/structure/HyperTree.h:444      NodeIdForPositionGPU
+ *   hyperacorn/csrc/modules/IndirectGridSample2D.h:24  IndirectGridSample2D
+ *   hyperacorn/csrc/modules/IndirectGridSample1D.h:24  IndirectGridSample1D
+ *   hyperacorn/csrc/modules/GradientCorrection.h       GradientCorrection
+ *   hyperacorn/csrc/geometry/geometry_tensor_qo.h:32   SampleVolumeIndirect
+ *   hyperacorn/csrc/geometry/Modules.h:23              FCBlock (+ DecodeFeatures)
+ *   hyperacorn/csrc/geometry/geometry.h:269-270        IntegrateSamplesXRay
+ *   hyperacorn/csrc/geometry/geometry.h:326-327        AccumulateSampleLossPerNode
+ *   hyperacorn/csrc/geometry/geometry.h:335            ComputeImage (fused form)
+ */
+#ifndef ATDF_H
+#define ATDF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same type as cudaStream_t. */
+typedef struct CUstream_st* atdf_stream_t;
+
+typedef enum {
+    ATDF_OK = 0,
+    ATDF_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size or shape */
+    ATDF_ERR_UNSUPPORTED = 2,      /* a configuration this build does not implement */
+    ATDF_ERR_WORKSPACE = 3,        /* workspace smaller than the queried size */
+    ATDF_ERR_CUDA = 4              /* a CUDA launch failed (cudaGetLastError) */
+} atdf_status;
+
+/* Bits OR-ed into *dev_error by kernels. */
+#define ATDF_DEVERR_HIT_OVERFLOW 0x1   /* a ray hit more than ATDF_MAX_HITS leaves */
+#define ATDF_DEVERR_SEG_CAPACITY 0x2   /* segment output capacity exceeded */
+#define ATDF_DEVERR_SAMPLE_CAPACITY 0x4 /* sample output capacity exceeded */
+#define ATDF_DEVERR_INDEX 0x8          /* an index outside its array (access skipped) */
+#define ATDF_DEVERR_TREE 0x10          /* tree flags did not converge / malformed tree */
+
+/* Largest number of leaves one ray may cross (the reference's limit,
+ * HyperTree.cu:280, max_intersections = 256). */
+#define ATDF_MAX_HITS 256
+
+#define ATDF_MAX_LAYERS 8
+
+/* Activations (Saiga ActivationFromString names used by FCBlock and
+ * DecodeFeatures; softplus uses softplus_beta and torch's threshold 20). */
+typedef enum {
+    ATDF_ACT_ID = 0,
+    ATDF_ACT_RELU = 1,
+    ATDF_ACT_SILU = 2,
+    ATDF_ACT_SIGMOID = 3,
+    ATDF_ACT_SOFTPLUS = 4,
+    ATDF_ACT_LEAKYRELU = 5,
+    ATDF_ACT_ABS = 6,
+    ATDF_ACT_TANH = 7
+} atdf_activation;
+
+typedef enum { ATDF_F32 = 0, ATDF_BF16 = 1 } atdf_dtype;
+
+/* HyperTree buffers (HyperTree.h:522-556), device pointers. node_flags comes
+ * from atdf_tree_flags: bit 0 = active leaf, bit 1 = subtree holds an active
+ * leaf. Children are -1 where absent; a child's box lies inside its parent's
+ * (HyperTree.cpp settree), which the ray traversal relies on. */
+typedef struct {
+    const float* node_position_min; /* [num_nodes, 3] */
+    const float* node_position_max; /* [num_nodes, 3] */
+    const int32_t* node_children;   /* [num_nodes, ns] */
+    const int32_t* node_active;     /* [num_nodes] */
+    const uint8_t* node_flags;      /* [num_nodes] */
+    int64_t num_nodes;
+    int32_t ns; /* 8 (octree) or 4 (quad tree) */
+    int32_t max_depth;
+} atdf_tree_t;
+
+/* Ray/leaf segments in canonical order: ray-major, and within a ray by
+ * (tmin, node id). Segment arrays have `capacity` entries. totals (device,
+ * 4 x int64): [0] segments, [1] samples, [2] max samples of one ray,
+ * [3] max segments of one ray. */
+typedef struct {
+    int64_t* ray_seg_offset;    /* [num_rays + 1] */
+    int64_t* ray_sample_offset; /* [num_rays + 1] */
+    int32_t* node;              /* leaf node id */
+    float* tmin;
+    float* tmax;
+    int32_t* nsamp;             /* samples in the segment */
+    int32_t* ray;               /* ray index */
+    int32_t* first;             /* index of the first sample within its ray */
+    int64_t capacity;
+    int64_t* totals;
+} atdf_segments_t;
+
+/* Vector-matrix factor field of GeometryTensorQO (geometry_tensor_qo.cpp:
+ * 257-380). Planes m = yz, xz, xy are stored channels-last:
+ * plane[m][slot][h][w][c] (the reference's [N, C, H, W] with C innermost);
+ * lines m = x, y, z are line[m][l][c] (the reference's [1, C, L, 1] with C
+ * innermost). leaf_slot maps a node id to its plane slot, -1 outside the ROI
+ * (whose features are zero, as in the reference with a ground-truth volume).
+ * mode 0 = "add" (F = C features), 1 = "cat" (F = 3C). */
+typedef struct {
+    int32_t channels;
+    int32_t mode;
+    int32_t dtype; /* atdf_dtype of planes and lines */
+    const void* plane[3];
+    int32_t plane_h[3];
+    int32_t plane_w[3];
+    const void* line[3];
+    int32_t line_len[3];
+    const int64_t* leaf_slot; /* [num_nodes] */
+    int64_t num_slots;
+    float roi_min[3];
+    float roi_max[3];
+} atdf_field_t;
+
+/* FP32 gradients of the field, same channels-last layouts as atdf_field_t. */
+typedef struct {
+    float* plane[3];
+    float* line[3];
+} atdf_field_grad_t;
+
+/* Decoder MLP (FCBlock): layers y = act(x W^T + b); the hidden activation
+ * follows every layer but the last, the last activation (DecodeFeatures)
+ * follows the last. weight[l] is [dims[l+1], dims[l]] (torch Linear). */
+typedef struct {
+    int32_t num_layers;
+    int32_t dims[ATDF_MAX_LAYERS + 1];
+    const float* weight[ATDF_MAX_LAYERS];
+    const float* bias[ATDF_MAX_LAYERS];
+    int32_t hidden_activation;
+    int32_t last_activation;
+    float softplus_beta;
+} atdf_mlp_t;
+
+typedef struct {
+    float* weight[ATDF_MAX_LAYERS];
+    float* bias[ATDF_MAX_LAYERS];
+} atdf_mlp_grad_t;
+
+const char* atdf_status_string(int status);
+int atdf_version(void);
+
+/* ---- HyperTree ----------------------------------------------------------
+ * node_flags for atdf_tree_t. No reference counterpart (the reference tests
+ * every active leaf per ray, HyperTree.cu:320-359); see atdf_ray_segments. */
+int atdf_tree_flags(const int32_t* node_active, const int32_t* node_children, int32_t ns, int64_t num_nodes,
+                    uint8_t* node_flags, int32_t* dev_error, atdf_stream_t stream);
+
+/* Replaces the intersection half of ComputeRaySamples
+ * (hyperacorn/csrc/structure/HyperTree.cu:266-371, launched from
+ * CreateSamplesForRays, HyperTree.cu:516-553): all active leaves hit by each
+ * ray (IntersectBoxRayPrecise, HyperTree.h:338-380; hits shorter than 1e-5
+ * skipped), with n = ceil(|tmax - tmin| / |box diagonal| * max_samples_per_node)
+ * samples each. Found by a descent of the tree that tests exactly the leaves
+ * the reference tests (a child's box lies inside its parent's). */
+int atdf_ray_segments(const atdf_tree_t* tree, const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                      int32_t max_samples_per_node, const atdf_segments_t* segs, int32_t* dev_error,
+                      atdf_stream_t stream);
+
+/* Replaces the sample half of ComputeRaySamples (HyperTree.cu:434-513) and
+ * the position recomputation of CreateSamplesForRays (HyperTree.cu:558-603):
+ * writes the SampleList arrays in canonical order. sample_rnd (nullable,
+ * [num_samples]) is the interval jitter; without it, jitter_seed != 0 draws
+ * it from the hash shared with the fused path, and jitter_seed == 0 uses the
+ * midpoint. Outputs have sample_capacity entries. */
+int atdf_emit_samples(const atdf_segments_t* segs, int64_t num_rays, const float* ray_origin,
+                      const float* ray_direction, const float* sample_rnd, uint64_t jitter_seed, float* out_position,
+                      float* out_t, float* out_weight, int64_t* out_ray_index, int64_t* out_local_index,
+                      int64_t* out_node_id, int64_t sample_capacity, int32_t* dev_error, atdf_stream_t stream);
+
+/* ComputeLocalSamples (HyperTree.cu:237-259): (x - min) / (max - min) * 2 - 1.
+ * group > 1: point i uses node[i / group] (the [G, g, 3] + [G] form). */
+int atdf_local_samples(const float* position, const int64_t* node, int64_t num_points, int64_t group,
+                       const float* node_position_min, const float* node_position_max, int64_t num_nodes,
+                       float* out_local, int32_t* dev_error, atdf_stream_t stream);
+
+/* NodeIdForPositionGPU (HyperTree.cu:1339-1400,1468-1525). */
+int atdf_node_id_for_position(const atdf_tree_t* tree, const int64_t* active_node_ids, const float* position,
+                              int64_t num_points, int64_t* out_node_id, float* out_mask, int32_t* dev_error,
+                              atdf_stream_t stream);
+
+/* ---- gathers (IndirectGridSample2D.cu / IndirectGridSample1D.cu) --------
+ * grid is [N, C, H, W] (1D: [N, C, W, 1]) with arbitrary element strides
+ * grid_stride = {sN, sC, sH, sW}. align_corners = True, border clamp.
+ * Backward ACCUMULATES into grad_grid (contiguous [N, C, H, W]) and grad_uv. */
+int atdf_grid_sample2d_forward(const float* grid, int64_t N, int64_t C, int64_t H, int64_t W,
+                               const int64_t* grid_stride, const int64_t* index, const float* uv, int64_t num_samples,
+                               float* out, int32_t* dev_error, atdf_stream_t stream);
+int atdf_grid_sample2d_backward(const float* grid, int64_t N, int64_t C, int64_t H, int64_t W,
+                                const int64_t* grid_stride, const int64_t* index, const float* uv,
+                                int64_t num_samples, const float* grad_out, float* grad_grid, float* grad_uv,
+                                int32_t* dev_error, atdf_stream_t stream);
+int atdf_grid_sample1d_forward(const float* grid, int64_t N, int64_t C, int64_t W, const int64_t* grid_stride,
+                               const int64_t* index, const float* uv, int64_t num_samples, float* out,
+                               int32_t* dev_error, atdf_stream_t stream);
+int atdf_grid_sample1d_backward(const float* grid, int64_t N, int64_t C, int64_t W, const int64_t* grid_stride,
+                                const int64_t* index, const float* uv, int64_t num_samples, const float* grad_out,
+                                float* grad_grid, float* grad_uv, int32_t* dev_error, atdf_stream_t stream);
+
+/* GradientCorrection backward (GradientCorrection.cu:22-48): g - (g.d) d. */
+int atdf_gradient_correction_backward(const float* ray_direction, const int64_t* ray_index, int64_t num_rays,
+                                      const float* grad_in, int64_t num_samples, float* grad_out, int32_t* dev_error,
+                                      atdf_stream_t stream);
+
+/* ---- field / decoder / integral (unfused SampleVolumeIndirect path) ---- */
+/* SampleVolumeIndirect_feature (geometry_tensor_qo.cpp:257-380), FP32 field:
+ * features [S, F] at sample positions in node ids. */
+int atdf_vm_features_forward(const atdf_field_t* field, const float* node_position_min,
+                             const float* node_position_max, int64_t num_nodes, const float* position,
+                             const int64_t* node_id, int64_t num_samples, float* out_features, int32_t* dev_error,
+                             atdf_stream_t stream);
+/* Adjoint of the above: ACCUMULATES into grad (FP32, channels-last). */
+int atdf_vm_features_backward(const atdf_field_t* field, const float* node_position_min,
+                              const float* node_position_max, int64_t num_nodes, const float* position,
+                              const int64_t* node_id, int64_t num_samples, const float* grad_features,
+                              const atdf_field_grad_t* grad, int32_t* dev_error, atdf_stream_t stream);
+
+/* FCBlock::forward (Modules.h:137) + DecodeFeatures last activation
+ * (geometry.cpp:176-253): out [S, dims[num_layers]]. Hidden widths <= 256. */
+int atdf_mlp_forward(const atdf_mlp_t* mlp, const float* x, int64_t num_rows, float* out, atdf_stream_t stream);
+/* Adjoint: writes grad_x [S, dims[0]] (nullable), ACCUMULATES grad. */
+int atdf_mlp_backward(const atdf_mlp_t* mlp, const float* x, int64_t num_rows, const float* grad_out, float* grad_x,
+                      const atdf_mlp_grad_t* grad, atdf_stream_t stream);
+
+/* IntegrateSamplesXRay (geometry.cpp:977-1019): ACCUMULATES
+ * image[c, ray[s]] += values[s, c] * weight[s]; image is [C, num_rays]. */
+int atdf_integrate_xray(const float* values, const float* weight, const int64_t* ray_index, int64_t num_samples,
+                        int32_t channels, int64_t num_rays, float* image, int32_t* dev_error, atdf_stream_t stream);
+
+/* AccumulateSampleLossPerNode (geometry.cpp:33-53) in FP64: ACCUMULATES
+ * loss_sum[node[s]] += mean_c(per_ray_loss[c, ray[s]]) * weight[s] and
+ * weight_sum[node[s]] += weight[s]. */
+int atdf_accumulate_loss_per_node(const float* per_ray_loss, int32_t channels, int64_t num_rays,
+                                  const int64_t* ray_index, const int64_t* node_id, const float* weight,
+                                  int64_t num_samples, int64_t num_nodes, double* loss_sum, double* weight_sum,
+                                  int32_t* dev_error, atdf_stream_t stream);
+
+/* ---- fused projection (ComputeImage with CreateSamplesForRays,
+ * SampleVolumeIndirect, DecodeFeatures and IntegrateSamplesXRay in one
+ * leaf-major pass; geometry.cpp:828-914) -------------------------------- */
+
+/* Workspace for the fused entry points, for num_rays rays through a tree of
+ * max_depth with num_slots plane slots. The workspace carries the ray/leaf
+ * segments from atdf_project_forward to atdf_project_backward and
+ * atdf_project_node_error: pass the same workspace, rays and tree to them. */
+int atdf_project_workspace_size(int64_t num_rays, int32_t max_depth, int32_t ns, int64_t num_slots,
+                                int32_t out_channels, size_t* bytes);
+
+/* Forward projection image [Cout, num_rays] (Cout = mlp->dims[last]).
+ * jitter_seed = 0: midpoint samples; else the interval jitter hash. */
+int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                         const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                         int32_t max_samples_per_node, uint64_t jitter_seed, float* image, void* workspace,
+                         size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
+
+/* Hand-written adjoint of atdf_project_forward given grad_image [Cout, R]:
+ * OVERWRITES grad_field (FP32, channels-last) and grad_mlp. Recomputes every
+ * sample (no stored activations); reuses the forward's segments from the
+ * workspace. */
+int atdf_project_backward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                          const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                          int32_t max_samples_per_node, uint64_t jitter_seed, const float* grad_image,
+                          const atdf_field_grad_t* grad_field, const atdf_mlp_grad_t* grad_mlp, void* workspace,
+                          size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
+
+/* Mean-squared-error loss of image [Cout, R] against target and its gradient:
+ * loss (device double) = scale * mean((image - target)^2), grad_image =
+ * scale * 2 (image - target) / (Cout R); per_ray_loss [Cout, R] (nullable)
+ * = (image - target)^2 (hyper_train.cpp:1019-1069, MSE branch). */
+int atdf_mse_loss(const float* image, const float* target, int64_t count, float scale, double* loss,
+                  float* grad_image, float* per_ray_loss, atdf_stream_t stream);
+
+/* Node-error scoring after atdf_project_forward (same workspace): OVERWRITES
+ * loss_sum / weight_sum [num_nodes] with the FP64 per-node sums of
+ * AccumulateSampleLossPerNode for per_ray_loss [Cout, R]. */
+int atdf_project_node_error(const atdf_tree_t* tree, const float* ray_origin, const float* ray_direction,
+                            int64_t num_rays, int32_t max_samples_per_node, uint64_t jitter_seed,
+                            const float* per_ray_loss, int32_t out_channels, double* loss_sum, double* weight_sum,
+                            void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATDF_H */
