@@ -3,6 +3,8 @@
 // reference-facing surface; this file only exposes it.
 #include <torch/extension.h>
 
+#include <optional>
+
 #include "atdf_host.h"
 
 namespace py = pybind11;
@@ -64,8 +66,12 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def("RaySegments", &HyperTreeBase::RaySegments)
         .def("CreateSamplesForRays", &HyperTreeBase::CreateSamplesForRays, py::arg("rays"),
              py::arg("max_samples_per_node"), py::arg("interval_jitter"))
-        .def("CreateSamplesForRaysWithRnd", &HyperTreeBase::CreateSamplesForRaysWithRnd, py::arg("rays"),
-             py::arg("max_samples_per_node"), py::arg("rnd"), py::arg("jitter_seed") = 0)
+        .def(
+            "CreateSamplesForRaysWithRnd",
+            [](HyperTreeBase& t, const RayList& rays, int M, std::optional<torch::Tensor> rnd, uint64_t seed) {
+                return t.CreateSamplesForRaysWithRnd(rays, M, rnd ? *rnd : torch::Tensor(), seed);
+            },
+            py::arg("rays"), py::arg("max_samples_per_node"), py::arg("rnd"), py::arg("jitter_seed") = 0)
         .def("ComputeLocalSamples", &HyperTreeBase::ComputeLocalSamples)
         .def("NodeIdForPositionGPU", &HyperTreeBase::NodeIdForPositionGPU)
         .def("SetErrorForActiveNodes", &HyperTreeBase::SetErrorForActiveNodes)
