@@ -477,10 +477,12 @@ int atdf_emit_samples(const atdf_segments_t* segs, int64_t num_rays, const float
                       float* out_t, float* out_weight, int64_t* out_ray_index, int64_t* out_local_index,
                       int64_t* out_node_id, int64_t sample_capacity, int32_t* dev_error, atdf_stream_t stream)
 {
-    if (!segs || num_rays < 0 || !out_position || !out_t || !out_weight || !out_ray_index || !out_local_index ||
-        !out_node_id)
-        return ATDF_ERR_INVALID_ARGUMENT;
+    if (!segs || num_rays < 0) return ATDF_ERR_INVALID_ARGUMENT;
     if (num_rays == 0) return ATDF_OK;
+    // with no capacity the outputs may be null; the kernel only flags overflow
+    if (sample_capacity > 0 &&
+        (!out_position || !out_t || !out_weight || !out_ray_index || !out_local_index || !out_node_id))
+        return ATDF_ERR_INVALID_ARGUMENT;
     const int64_t threads = num_rays * 32;
     emit_samples_kernel<<<(unsigned)div_up(threads, 256), 256, 0, (cudaStream_t)stream>>>(
         *segs, num_rays, ray_origin, ray_direction, sample_rnd, jitter_seed, out_position, out_t, out_weight,
