@@ -136,6 +136,8 @@ def _declare(L):
                                         P, ct.POINTER(FieldGrad), ct.POINTER(MlpGrad), P, SZ, P, P]),
         "atdf_mse_loss": (I32, [P, P, I64, F32, P, P, P, P]),
         "atdf_project_node_error": (I32, [ct.POINTER(Tree), P, P, I64, I32, U64, P, I32, P, P, P, SZ, P, P]),
+        "atdf_project_forward_noalloc": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, I32,
+                                               U64, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

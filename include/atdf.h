@@ -291,6 +291,25 @@ int atdf_project_node_error(const atdf_tree_t* tree, const float* ray_origin, co
                             const float* per_ray_loss, int32_t out_channels, double* loss_sum, double* weight_sum,
                             void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
 
+/* ---- forward projection without device allocation ----------------------
+ * No counterpart in the reference (it allocates with torch on every call).
+ * For callers that cannot call cudaMalloc (a plugin whose host framework owns
+ * every device allocation, or a loop where an allocation would synchronise
+ * the device): atdf_project_forward with its workspace taken from a static
+ * device array of ATDF_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading
+ * the library holds until exit. A problem whose workspace
+ * (atdf_project_workspace_size) exceeds it is rejected with
+ * ATDF_ERR_WORKSPACE before any launch; at depth 4 that is about 10,000
+ * rays per call. The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture. All calls share the array: calls that overlap on the GPU
+ * race. Inputs and outputs are the caller's, as in atdf_project_forward. */
+#define ATDF_NOALLOC_SCRATCH_BYTES (16u << 20)
+int atdf_project_forward_noalloc(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                 const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                 int32_t max_samples_per_node, uint64_t jitter_seed, float* image,
+                                 int32_t* dev_error, atdf_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
