@@ -128,6 +128,24 @@ __device__ __forceinline__ float local_coord(float x, float mn, float mx)
     return __fsub_rn(__fmul_rn(b, 2.0f), 1.0f);
 }
 
+// Same value as local_coord when inv_size is nonzero: it is only set when the
+// size is a power of two, and then (x - mn) / size and (x - mn) * (1 / size)
+// are the same exact scaling.
+__device__ __forceinline__ float local_coord_fast(float x, float mn, float size, float inv_size)
+{
+    float a = __fsub_rn(x, mn);
+    float b = inv_size != 0.0f ? __fmul_rn(a, inv_size) : __fdiv_rn(a, size);
+    return __fsub_rn(__fmul_rn(b, 2.0f), 1.0f);
+}
+
+// 1 / x when x is a power of two (exactly representable reciprocal), else 0.
+__host__ __device__ __forceinline__ float pow2_reciprocal(float x)
+{
+    int e = 0;
+    const float m = frexpf(x, &e);
+    return (x > 0.0f && m == 0.5f) ? ldexpf(1.0f, 1 - e) : 0.0f;
+}
+
 // ROI-normalised x line coordinate (geometry_tensor_qo.cpp:293).
 __device__ __forceinline__ float roi_coord(float x, float rmin, float rmax)
 {
@@ -148,8 +166,9 @@ struct Corner2 {
 __device__ __forceinline__ Corner2 corners2(float u, float v, int H, int W)
 {
     Corner2 c;
-    float ix = __fmul_rn(__fdiv_rn(__fadd_rn(u, 1.0f), 2.0f), (float)(W - 1));
-    float iy = __fmul_rn(__fdiv_rn(__fadd_rn(v, 1.0f), 2.0f), (float)(H - 1));
+    // (u + 1) / 2 as a multiplication by 0.5: both round the same exact value
+    float ix = __fmul_rn(__fmul_rn(__fadd_rn(u, 1.0f), 0.5f), (float)(W - 1));
+    float iy = __fmul_rn(__fmul_rn(__fadd_rn(v, 1.0f), 0.5f), (float)(H - 1));
     int x0 = (int)floorf(ix), y0 = (int)floorf(iy);
     int x1 = x0 + 1, y1 = y0 + 1;
     c.fx0 = (float)x0;
@@ -177,7 +196,7 @@ struct Corner1 {
 __device__ __forceinline__ Corner1 corners1(float u, int W)
 {
     Corner1 c;
-    float ix = __fmul_rn(__fdiv_rn(__fadd_rn(u, 1.0f), 2.0f), (float)(W - 1));
+    float ix = __fmul_rn(__fmul_rn(__fadd_rn(u, 1.0f), 0.5f), (float)(W - 1));
     int x0 = (int)floorf(ix);
     c.fx0 = (float)x0;
     c.fx1 = (float)(x0 + 1);
@@ -232,7 +251,9 @@ __device__ __forceinline__ SampleGeo sample_geo(const float p[3], const float* b
 // ---------------------------------------------------------------------------
 // Activations (FCBlock hidden activation, DecodeFeatures last activation).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf(-x)); }
+// Logistic function with the fast exponential and divide intrinsics (a few
+// ulp; the decoder tolerance is 1e-5 relative).
+__device__ __forceinline__ float sigmoidf_(float x) { return __fdividef(1.0f, 1.0f + __expf(-x)); }
 
 __device__ __forceinline__ float act_fwd(int a, float x, float beta)
 {

@@ -38,6 +38,7 @@ constexpr int kT = 32;                // samples per tile
 constexpr int kSPT = kThreads / kT;   // threads per sample
 constexpr int kSegItem = 64;          // segments per work item
 constexpr int kLineWin = 64;          // line-gradient window entries per line
+constexpr int kSegTabArrays = 18;     // arrays of the per-item segment table
 
 // ---------------------------------------------------------------------------
 // workspace
@@ -250,12 +251,29 @@ struct Map {
     static_assert(PER >= 1 && RM * CN == PER && TX * TY == kThreads && N % CN == 0 && M % RM == 0, "tile map");
 };
 
-template <int M, int N>
+// Thread coordinates of the tile map. RF (row-fast): consecutive threads own
+// consecutive output rows, which makes k-major ([col][row]) epilogue stores
+// conflict-free; otherwise consecutive threads own consecutive columns.
+template <int M, int N, bool RF>
+__device__ __forceinline__ void tile_coords(int& tx, int& ty)
+{
+    using Mp = Map<M, N>;
+    if (RF) {
+        ty = threadIdx.x % Mp::TY;
+        tx = threadIdx.x / Mp::TY;
+    } else {
+        tx = threadIdx.x % Mp::TX;
+        ty = threadIdx.x / Mp::TX;
+    }
+}
+
+template <int M, int N, bool RF = false>
 __device__ __forceinline__ void gemm(float (&acc)[Map<M, N>::RM][Map<M, N>::CN], const float* At, int lda,
                                      const float* Bt, int ldb, int K)
 {
     using Mp = Map<M, N>;
-    const int tx = threadIdx.x % Mp::TX, ty = threadIdx.x / Mp::TX;
+    int tx, ty;
+    tile_coords<M, N, RF>(tx, ty);
     const float* a = At + ty * Mp::RM;
     const float* b = Bt + tx * Mp::CN;
 #pragma unroll 4
@@ -296,6 +314,7 @@ struct FusedParams {
     atdf_mlp_grad_t gmlp;
     int32_t* err;
     int plane_off[4];  // float offsets of the three planes in shared memory (+ total)
+    float roi_inv;     // 1 / (roi_max.x - roi_min.x) when a power of two, else 0
 };
 
 template <int C, int MODE, int H, int NH>
@@ -362,7 +381,7 @@ struct Smem {
         sseg = o;
         o += kT;
         segi = o;
-        o += 8 * (kSegItem + 4);
+        o += kSegTabArrays * (kSegItem + 4);
         total = o;
     }
 };
@@ -376,21 +395,32 @@ struct SegTab {
     int* id;
     float* tmin;
     float* tmax;
-    float* acc;  // forward partial integral / backward dI of the ray
+    float* step;  // (tmax - tmin) / n
+    float* acc;   // forward partial integral / backward dI of the ray
+    float* bmin[3];
+    float* size[3];
+    float* inv[3];  // 1 / size when size is a power of two, else 0
 };
 
 __device__ __forceinline__ SegTab seg_tab(float* base)
 {
+    constexpr int S = kSegItem + 4;
     SegTab t;
     int* ib = reinterpret_cast<int*>(base);
     t.start = ib;
-    t.ray = ib + (kSegItem + 4);
-    t.node = ib + 2 * (kSegItem + 4);
-    t.n = ib + 3 * (kSegItem + 4);
-    t.id = ib + 4 * (kSegItem + 4);
-    t.tmin = base + 5 * (kSegItem + 4);
-    t.tmax = base + 6 * (kSegItem + 4);
-    t.acc = base + 7 * (kSegItem + 4);
+    t.ray = ib + S;
+    t.node = ib + 2 * S;
+    t.n = ib + 3 * S;
+    t.id = ib + 4 * S;
+    t.tmin = base + 5 * S;
+    t.tmax = base + 6 * S;
+    t.step = base + 7 * S;
+    t.acc = base + 8 * S;
+    for (int k = 0; k < 3; ++k) {
+        t.bmin[k] = base + (9 + k) * S;
+        t.size[k] = base + (12 + k) * S;
+        t.inv[k] = base + (15 + k) * S;
+    }
     return t;
 }
 
@@ -454,9 +484,20 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
         tab.ray[tid] = w.ray[sid];
         tab.node[tid] = w.node[sid];
         tab.n[tid] = w.nsamp[sid];
-        tab.tmin[tid] = w.tmin[sid];
-        tab.tmax[tid] = w.tmax[sid];
+        const float tmin = w.tmin[sid], tmax = w.tmax[sid];
+        const int n = w.nsamp[sid], node = w.node[sid];
+        tab.tmin[tid] = tmin;
+        tab.tmax[tid] = tmax;
+        tab.step[tid] = __fdiv_rn(__fsub_rn(tmax, tmin), (float)n);  // sample_t's step
         tab.acc[tid] = want_dI ? p.grad_image[w.ray[sid]] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
+            const float sz = __fsub_rn(mx, mn);
+            tab.bmin[k][tid] = mn;
+            tab.size[k][tid] = sz;
+            tab.inv[k][tid] = pow2_reciprocal(sz);
+        }
     }
     __syncthreads();
     if (tid < 32) {
@@ -502,6 +543,15 @@ __device__ __forceinline__ int find_seg(const SegTab& tab, int nseg, int k)
     return lo;
 }
 
+// sample_t with the segment's step precomputed (same operations).
+__device__ __forceinline__ float sample_t_step(float tmin, float step, int j, float a)
+{
+    const float t1 = __fadd_rn(tmin, __fmul_rn((float)j, step));
+    const float t2 = __fadd_rn(tmin, __fmul_rn((float)(j + 1), step));
+    const float oma = __fsub_rn(1.0f, a);
+    return __fadd_rn(__fmul_rn(t1, oma), __fmul_rn(t2, a));
+}
+
 __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const SegTab& tab, int nseg, int k)
 {
     SampleState s;
@@ -510,14 +560,40 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
     const int n = tab.n[s.si];
     const int r = tab.ray[s.si];
     s.node = tab.node[s.si];
-    const float tmin = tab.tmin[s.si], tmax = tab.tmax[s.si];
-    const float t = sample_t(tmin, tmax, n, j, sample_a(nullptr, 0, p.seed, r, s.node, j));
-    const float tp = j > 0 ? sample_t(tmin, tmax, n, j - 1, sample_a(nullptr, 0, p.seed, r, s.node, j - 1)) : 0.0f;
-    const float tn = j < n - 1 ? sample_t(tmin, tmax, n, j + 1, sample_a(nullptr, 0, p.seed, r, s.node, j + 1)) : 0.0f;
+    const float tmin = tab.tmin[s.si], tmax = tab.tmax[s.si], step = tab.step[s.si];
+    const float t = sample_t_step(tmin, step, j, sample_a(nullptr, 0, p.seed, r, s.node, j));
+    const float tp = j > 0 ? sample_t_step(tmin, step, j - 1, sample_a(nullptr, 0, p.seed, r, s.node, j - 1)) : 0.0f;
+    const float tn =
+        j < n - 1 ? sample_t_step(tmin, step, j + 1, sample_a(nullptr, 0, p.seed, r, s.node, j + 1)) : 0.0f;
     s.w = sample_w(tmin, tmax, n, j, tp, t, tn);
 #pragma unroll
     for (int k2 = 0; k2 < 3; ++k2) s.pos[k2] = __fadd_rn(p.origin[3 * r + k2], __fmul_rn(p.dir[3 * r + k2], t));
     return s;
+}
+
+// sample_geo with the segment's box from the table and division-free
+// coordinates where the divisor is a power of two (bit-identical).
+__device__ __forceinline__ SampleGeo sample_geo_fast(const FusedParams& p, const SegTab& tab, int si,
+                                                     const float pos[3])
+{
+    float loc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) loc[k] = local_coord_fast(pos[k], tab.bmin[k][si], tab.size[k][si], tab.inv[k][si]);
+    SampleGeo g;
+    g.pu[0] = loc[1];
+    g.pv[0] = loc[2];
+    g.pu[1] = loc[0];
+    g.pv[1] = loc[2];
+    g.pu[2] = loc[0];
+    g.pv[2] = loc[1];
+    const float a = __fsub_rn(pos[0], p.field.roi_min[0]);
+    const float b = __fmul_rn(2.0f, a);
+    const float c = p.roi_inv != 0.0f ? __fmul_rn(b, p.roi_inv)
+                                      : __fdiv_rn(b, __fsub_rn(p.field.roi_max[0], p.field.roi_min[0]));
+    g.lu[0] = __fsub_rn(c, 1.0f);
+    g.lu[1] = loc[1];
+    g.lu[2] = pos[2];
+    return g;
 }
 
 // Gathered values of one sample for channels q*CPT .. q*CPT+CPT-1.
@@ -607,12 +683,13 @@ __device__ void load_weights(const FusedParams& p, float* sm, const Smem<C, MODE
 
 // Epilogue of a forward layer: pre = acc + b; writes act(pre) k-major (and
 // the pre-activation / a sample-major copy when requested).
-template <int M, int N>
+template <int M, int N, bool RF = false>
 __device__ __forceinline__ void store_layer(const float (&acc)[Map<M, N>::RM][Map<M, N>::CN], const float* bias,
                                             int act, float beta, float* out_t, float* pre_t, float* out_s)
 {
     using Mp = Map<M, N>;
-    const int tx = threadIdx.x % Mp::TX, ty = threadIdx.x / Mp::TX;
+    int tx, ty;
+    tile_coords<M, N, RF>(tx, ty);
 #pragma unroll
     for (int i = 0; i < Mp::RM; ++i)
 #pragma unroll
@@ -694,9 +771,7 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
                 w = st.w;
                 si = st.si;
                 if (real) {
-                    float bmin[3], bmax[3];
-                    item_box(p, st.node, bmin, bmax);
-                    const SampleGeo g = sample_geo(st.pos, bmin, bmax, p.field.roi_min, p.field.roi_max);
+                    const SampleGeo g = sample_geo_fast(p, tab, st.si, st.pos);
                     Gathered<CPT> ga;
                     gather_sample<C, CPT>(p, sm, g, q, ga);
                     features_of<C, MODE, CPT>(ga, f);
@@ -714,16 +789,16 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
             {
                 float acc[Map<kT, H>::RM][Map<kT, H>::CN];
                 zero<kT, H>(acc);
-                gemm<kT, H>(acc, sm + L.xt, kT, sm + L.w0t, H, F);
-                store_layer<kT, H>(acc, sm + L.b0, hact, beta, sm + L.h0t, nullptr, nullptr);
+                gemm<kT, H, true>(acc, sm + L.xt, kT, sm + L.w0t, H, F);
+                store_layer<kT, H, true>(acc, sm + L.b0, hact, beta, sm + L.h0t, nullptr, nullptr);
             }
             __syncthreads();
             const float* hlast = sm + L.h0t;
             if (NH == 2) {
                 float acc[Map<kT, H>::RM][Map<kT, H>::CN];
                 zero<kT, H>(acc);
-                gemm<kT, H>(acc, sm + L.h0t, kT, sm + L.w1t, H, H);
-                store_layer<kT, H>(acc, sm + L.b1, hact, beta, sm + L.a1t, nullptr, nullptr);
+                gemm<kT, H, true>(acc, sm + L.h0t, kT, sm + L.w1t, H, H);
+                store_layer<kT, H, true>(acc, sm + L.b1, hact, beta, sm + L.a1t, nullptr, nullptr);
                 __syncthreads();
                 hlast = sm + L.a1t;
             }
@@ -740,7 +815,7 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
 }
 
 template <int C, int MODE, int H, int NH>
-__global__ void __launch_bounds__(kThreads) fused_backward_kernel(FusedParams p)
+__global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams p)
 {
     using K = Cfg<C, MODE, H, NH>;
     constexpr int F = K::F, CPT = K::CPT, NF = MODE ? 3 * CPT : CPT;
@@ -807,14 +882,13 @@ __global__ void __launch_bounds__(kThreads) fused_backward_kernel(FusedParams p)
 #pragma unroll
             for (int i = 0; i < NF; ++i) f[i] = 0.0f;
             float w = 0.0f, dIw = 0.0f;
+            SampleGeo g;
             if (valid) {
                 const SampleState st = sample_state(p, tab, it.nseg, k);
                 w = st.w;
                 dIw = __fmul_rn(tab.acc[st.si], st.w);
                 if (real) {
-                    float bmin[3], bmax[3];
-                    item_box(p, st.node, bmin, bmax);
-                    const SampleGeo g = sample_geo(st.pos, bmin, bmax, p.field.roi_min, p.field.roi_max);
+                    g = sample_geo_fast(p, tab, st.si, st.pos);
                     Gathered<CPT> ga;
                     gather_sample<C, CPT>(p, sm, g, q, ga);
                     features_of<C, MODE, CPT>(ga, f);
@@ -837,8 +911,8 @@ __global__ void __launch_bounds__(kThreads) fused_backward_kernel(FusedParams p)
             {
                 float acc[Map<kT, H>::RM][Map<kT, H>::CN];
                 zero<kT, H>(acc);
-                gemm<kT, H>(acc, sm + L.xt, kT, sm + L.w0t, H, F);
-                store_layer<kT, H>(acc, sm + L.b0, hact, beta, sm + L.h0t, sm + L.a0t, sm + L.h0s);
+                gemm<kT, H, true>(acc, sm + L.xt, kT, sm + L.w0t, H, F);
+                store_layer<kT, H, true>(acc, sm + L.b0, hact, beta, sm + L.h0t, sm + L.a0t, sm + L.h0s);
             }
             __syncthreads();
             const float* hlast_s;
@@ -928,10 +1002,6 @@ __global__ void __launch_bounds__(kThreads) fused_backward_kernel(FusedParams p)
             __syncthreads();
             // scatter dX into the shared plane-gradient copy and line windows
             if (valid && real) {
-                const SampleState st = sample_state(p, tab, it.nseg, k);
-                float bmin[3], bmax[3];
-                item_box(p, st.node, bmin, bmax);
-                const SampleGeo g = sample_geo(st.pos, bmin, bmax, p.field.roi_min, p.field.roi_max);
                 const int c0 = q * CPT;
 #pragma unroll
                 for (int m = 0; m < 3; ++m) {
@@ -1117,6 +1187,7 @@ static int prepare(const atdf_tree_t* tree, const atdf_field_t* field, const atd
         off += field->plane_h[m] * field->plane_w[m] * field->channels;
     }
     p.plane_off[3] = off;
+    p.roi_inv = pow2_reciprocal(field->roi_max[0] - field->roi_min[0]);
     const size_t need = ws_layout(R, tree->max_depth, field->num_slots, nullptr, nullptr);
     if (ws_bytes < need) return ATDF_ERR_WORKSPACE;
     ws_layout(R, tree->max_depth, field->num_slots, (char*)workspace, &p.ws);

@@ -322,6 +322,7 @@ def run_ours(args, rank, world):
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
                      "algorithmic_bytes": dom_bytes, "kernel_ms": dom_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+        "kernels_ms": {"fused_forward_call": tf, "fused_backward_call": tb},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "samples_per_s": world * sg.num_samples / (ms * 1e-3),
