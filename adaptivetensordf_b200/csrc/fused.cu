@@ -26,7 +26,7 @@
 
 #include <algorithm>
 
-#include "atdf_common.cuh"
+#include "fused_common.cuh"
 
 namespace atdf {
 
@@ -36,100 +36,9 @@ int launch_ray_segments(const atdf_tree_t& tree, const float* origin, const floa
 constexpr int kThreads = 256;
 constexpr int kT = 32;                // samples per tile
 constexpr int kSPT = kThreads / kT;   // threads per sample
-constexpr int kSegItem = 64;          // segments per work item
-constexpr int kLineWin = 64;          // line-gradient window entries per line
-constexpr int kSegTabArrays = 18;     // arrays of the per-item segment table
-
-// ---------------------------------------------------------------------------
-// workspace
-// ---------------------------------------------------------------------------
-struct Ws {
-    int64_t* ray_seg_offset;
-    int64_t* ray_sample_offset;
-    int64_t* totals;
-    int32_t* node;
-    float* tmin;
-    float* tmax;
-    int32_t* nsamp;
-    int32_t* ray;
-    int32_t* first;
-    float* seg_partial;
-    int32_t* bucket;
-    int32_t* slot_offset;  // [nslot + 2]
-    int32_t* slot_cursor;  // [nslot + 1]
-    int32_t* item_offset;  // [nslot + 2]
-    int32_t* counters;     // [8]
-    int64_t cap;
-    int64_t nslot;
-};
-
-static int64_t seg_capacity(int64_t R, int max_depth)
-{
-    int64_t per = 3 * ((int64_t)1 << std::min(std::max(max_depth, 0), 20)) + 3;
-    per = std::min<int64_t>(per, ATDF_MAX_HITS);
-    return std::max<int64_t>(R * per, 1);
-}
-
-static size_t carve(char*& p, size_t bytes)
-{
-    size_t off = (size_t)p;
-    p += (bytes + 255) & ~(size_t)255;
-    return off;
-}
-
-// Lays the workspace out from base (nullptr: only the size).
-static size_t ws_layout(int64_t R, int max_depth, int64_t nslot, char* base, Ws* w)
-{
-    const int64_t cap = seg_capacity(R, max_depth);
-    char* p = base;
-    Ws x;
-    x.ray_seg_offset = (int64_t*)carve(p, (R + 1) * 8);
-    x.ray_sample_offset = (int64_t*)carve(p, (R + 1) * 8);
-    x.totals = (int64_t*)carve(p, 4 * 8);
-    x.node = (int32_t*)carve(p, cap * 4);
-    x.tmin = (float*)carve(p, cap * 4);
-    x.tmax = (float*)carve(p, cap * 4);
-    x.nsamp = (int32_t*)carve(p, cap * 4);
-    x.ray = (int32_t*)carve(p, cap * 4);
-    x.first = (int32_t*)carve(p, cap * 4);
-    x.seg_partial = (float*)carve(p, cap * 4);
-    x.bucket = (int32_t*)carve(p, cap * 4);
-    x.slot_offset = (int32_t*)carve(p, (nslot + 2) * 4);
-    x.slot_cursor = (int32_t*)carve(p, (nslot + 1) * 4);
-    x.item_offset = (int32_t*)carve(p, (nslot + 2) * 4);
-    x.counters = (int32_t*)carve(p, 8 * 4);
-    x.cap = cap;
-    x.nslot = nslot;
-    if (w) *w = x;
-    return (size_t)(p - base);
-}
-
-static atdf_segments_t ws_segments(const Ws& w)
-{
-    atdf_segments_t s;
-    s.ray_seg_offset = w.ray_seg_offset;
-    s.ray_sample_offset = w.ray_sample_offset;
-    s.node = w.node;
-    s.tmin = w.tmin;
-    s.tmax = w.tmax;
-    s.nsamp = w.nsamp;
-    s.ray = w.ray;
-    s.first = w.first;
-    s.capacity = w.cap;
-    s.totals = w.totals;
-    return s;
-}
-
 // ---------------------------------------------------------------------------
 // bucketing by plane slot
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int64_t seg_slot(const atdf_field_t& f, int64_t num_nodes, int32_t node)
-{
-    if (node < 0 || node >= num_nodes) return f.num_slots;
-    const int64_t s = f.leaf_slot[node];
-    return (s < 0 || s >= f.num_slots) ? f.num_slots : s;
-}
-
 __global__ void bucket_count_kernel(Ws w, atdf_field_t f, int64_t num_nodes)
 {
     const int64_t nseg = min(w.totals[0], w.cap);
@@ -171,52 +80,6 @@ __global__ void ray_reduce_kernel(Ws w, int64_t R, float* image)
         for (int64_t s = b; s < e; ++s) acc = __fadd_rn(acc, w.seg_partial[s]);
     image[r] = acc;
 }
-
-// ---------------------------------------------------------------------------
-// TMA bulk copies and a bounded mbarrier wait
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tma_bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait (about a second of try_wait rounds); false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase)
-{
-    for (int i = 0; i < (1 << 22); ++i)
-        if (mbar_try_wait(bar, phase)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // register-tiled shared-memory GEMM: acc[i][j] += sum_k A[k][row0+i] B[k][col0+j]
@@ -300,23 +163,6 @@ __device__ __forceinline__ void zero(float (&acc)[Map<M, N>::RM][Map<M, N>::CN])
 // ---------------------------------------------------------------------------
 // fused kernels
 // ---------------------------------------------------------------------------
-struct FusedParams {
-    atdf_tree_t tree;
-    atdf_field_t field;
-    atdf_mlp_t mlp;
-    const float* origin;
-    const float* dir;
-    int64_t R;
-    uint64_t seed;
-    Ws ws;
-    const float* grad_image;
-    atdf_field_grad_t gfield;
-    atdf_mlp_grad_t gmlp;
-    int32_t* err;
-    int plane_off[4];  // float offsets of the three planes in shared memory (+ total)
-    float roi_inv;     // 1 / (roi_max.x - roi_min.x) when a power of two, else 0
-};
-
 template <int C, int MODE, int H, int NH>
 struct Cfg {
     static constexpr int F = MODE ? 3 * C : C;
@@ -385,216 +231,6 @@ struct Smem {
         total = o;
     }
 };
-
-// Per-item segment table in shared memory.
-struct SegTab {
-    int* start;  // [kSegItem + 1]
-    int* ray;
-    int* node;
-    int* n;
-    int* id;
-    float* tmin;
-    float* tmax;
-    float* step;  // (tmax - tmin) / n
-    float* acc;   // forward partial integral / backward dI of the ray
-    float* bmin[3];
-    float* size[3];
-    float* inv[3];  // 1 / size when size is a power of two, else 0
-};
-
-__device__ __forceinline__ SegTab seg_tab(float* base)
-{
-    constexpr int S = kSegItem + 4;
-    SegTab t;
-    int* ib = reinterpret_cast<int*>(base);
-    t.start = ib;
-    t.ray = ib + S;
-    t.node = ib + 2 * S;
-    t.n = ib + 3 * S;
-    t.id = ib + 4 * S;
-    t.tmin = base + 5 * S;
-    t.tmax = base + 6 * S;
-    t.step = base + 7 * S;
-    t.acc = base + 8 * S;
-    for (int k = 0; k < 3; ++k) {
-        t.bmin[k] = base + (9 + k) * S;
-        t.size[k] = base + (12 + k) * S;
-        t.inv[k] = base + (15 + k) * S;
-    }
-    return t;
-}
-
-// Takes the next work item; fills the segment table; issues the plane TMA.
-// Returns the item's slot, or -1 when the queue is empty.
-struct ItemInfo {
-    int64_t slot;
-    int nseg;
-    int total;
-};
-
-__device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, float* sm, SegTab tab, uint64_t* bar,
-                                              int* s_ctl, bool want_dI)
-{
-    const Ws& w = p.ws;
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        const int nitems = w.item_offset[w.nslot + 1];
-        const int it = atomicAdd(&w.counters[queue], 1);
-        int slot = -1, b0 = 0, nseg = 0;
-        if (it < nitems) {
-            int lo = 0, hi = (int)w.nslot + 1;  // item_offset[lo] <= it < item_offset[hi]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (w.item_offset[mid] <= it)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            slot = lo;
-            b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * kSegItem;
-            const int b1 = min(b0 + kSegItem, w.slot_offset[slot + 1]);
-            nseg = b1 - b0;
-            if (slot < w.nslot) {
-                uint32_t bytes = 0;
-                for (int m = 0; m < 3; ++m)
-                    bytes += (uint32_t)(p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels * 4);
-                fence_proxy_async();
-                mbar_expect_tx(bar, bytes);
-                for (int m = 0; m < 3; ++m) {
-                    const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
-                    tma_bulk_load(sm + p.plane_off[m], (const float*)p.field.plane[m] + (int64_t)slot * pf,
-                                  (uint32_t)(pf * 4), bar);
-                }
-            }
-        }
-        s_ctl[0] = slot;
-        s_ctl[1] = b0;
-        s_ctl[2] = nseg;
-    }
-    __syncthreads();
-    ItemInfo info;
-    info.slot = s_ctl[0];
-    info.nseg = s_ctl[2];
-    info.total = 0;
-    if (info.slot < 0) return info;
-    const int b0 = s_ctl[1];
-    if (tid < info.nseg) {
-        const int sid = w.bucket[b0 + tid];
-        tab.id[tid] = sid;
-        tab.ray[tid] = w.ray[sid];
-        tab.node[tid] = w.node[sid];
-        tab.n[tid] = w.nsamp[sid];
-        const float tmin = w.tmin[sid], tmax = w.tmax[sid];
-        const int n = w.nsamp[sid], node = w.node[sid];
-        tab.tmin[tid] = tmin;
-        tab.tmax[tid] = tmax;
-        tab.step[tid] = __fdiv_rn(__fsub_rn(tmax, tmin), (float)n);  // sample_t's step
-        tab.acc[tid] = want_dI ? p.grad_image[w.ray[sid]] : 0.0f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
-            const float sz = __fsub_rn(mx, mn);
-            tab.bmin[k][tid] = mn;
-            tab.size[k][tid] = sz;
-            tab.inv[k][tid] = pow2_reciprocal(sz);
-        }
-    }
-    __syncthreads();
-    if (tid < 32) {
-        // exclusive scan of the sample counts (kSegItem = 64: two per lane)
-        const int i0 = 2 * tid, i1 = 2 * tid + 1;
-        const int v0 = i0 < info.nseg ? tab.n[i0] : 0;
-        const int v1 = i1 < info.nseg ? tab.n[i1] : 0;
-        int s = v0 + v1;
-        int incl = s;
-        for (int off = 1; off < 32; off <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, off);
-            if (tid >= off) incl += v;
-        }
-        const int ex = incl - s;
-        tab.start[i0] = ex;
-        tab.start[i1] = ex + v0;
-        if (tid == 31) tab.start[kSegItem] = incl;
-    }
-    __syncthreads();
-    info.total = tab.start[info.nseg];
-    return info;
-}
-
-// Geometry of sample k of the current item (computed by all 8 threads of the
-// sample): segment index, weight, position.
-struct SampleState {
-    int si;
-    float w;
-    float pos[3];
-    int node;
-};
-
-__device__ __forceinline__ int find_seg(const SegTab& tab, int nseg, int k)
-{
-    int lo = 0, hi = nseg;  // start[lo] <= k < start[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (tab.start[mid] <= k)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
-// sample_t with the segment's step precomputed (same operations).
-__device__ __forceinline__ float sample_t_step(float tmin, float step, int j, float a)
-{
-    const float t1 = __fadd_rn(tmin, __fmul_rn((float)j, step));
-    const float t2 = __fadd_rn(tmin, __fmul_rn((float)(j + 1), step));
-    const float oma = __fsub_rn(1.0f, a);
-    return __fadd_rn(__fmul_rn(t1, oma), __fmul_rn(t2, a));
-}
-
-__device__ __forceinline__ SampleState sample_state(const FusedParams& p, const SegTab& tab, int nseg, int k)
-{
-    SampleState s;
-    s.si = find_seg(tab, nseg, k);
-    const int j = k - tab.start[s.si];
-    const int n = tab.n[s.si];
-    const int r = tab.ray[s.si];
-    s.node = tab.node[s.si];
-    const float tmin = tab.tmin[s.si], tmax = tab.tmax[s.si], step = tab.step[s.si];
-    const float t = sample_t_step(tmin, step, j, sample_a(nullptr, 0, p.seed, r, s.node, j));
-    const float tp = j > 0 ? sample_t_step(tmin, step, j - 1, sample_a(nullptr, 0, p.seed, r, s.node, j - 1)) : 0.0f;
-    const float tn =
-        j < n - 1 ? sample_t_step(tmin, step, j + 1, sample_a(nullptr, 0, p.seed, r, s.node, j + 1)) : 0.0f;
-    s.w = sample_w(tmin, tmax, n, j, tp, t, tn);
-#pragma unroll
-    for (int k2 = 0; k2 < 3; ++k2) s.pos[k2] = __fadd_rn(p.origin[3 * r + k2], __fmul_rn(p.dir[3 * r + k2], t));
-    return s;
-}
-
-// sample_geo with the segment's box from the table and division-free
-// coordinates where the divisor is a power of two (bit-identical).
-__device__ __forceinline__ SampleGeo sample_geo_fast(const FusedParams& p, const SegTab& tab, int si,
-                                                     const float pos[3])
-{
-    float loc[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) loc[k] = local_coord_fast(pos[k], tab.bmin[k][si], tab.size[k][si], tab.inv[k][si]);
-    SampleGeo g;
-    g.pu[0] = loc[1];
-    g.pv[0] = loc[2];
-    g.pu[1] = loc[0];
-    g.pv[1] = loc[2];
-    g.pu[2] = loc[0];
-    g.pv[2] = loc[1];
-    const float a = __fsub_rn(pos[0], p.field.roi_min[0]);
-    const float b = __fmul_rn(2.0f, a);
-    const float c = p.roi_inv != 0.0f ? __fmul_rn(b, p.roi_inv)
-                                      : __fdiv_rn(b, __fsub_rn(p.field.roi_max[0], p.field.roi_min[0]));
-    g.lu[0] = __fsub_rn(c, 1.0f);
-    g.lu[1] = loc[1];
-    g.lu[2] = pos[2];
-    return g;
-}
 
 // Gathered values of one sample for channels q*CPT .. q*CPT+CPT-1.
 template <int CPT>
@@ -717,15 +353,6 @@ __device__ __forceinline__ float last_layer(const float* ht, const float* wl, fl
     acc += __shfl_xor_sync(0xffffffffu, acc, 2);
     acc += __shfl_xor_sync(0xffffffffu, acc, 1);
     return acc + bl;
-}
-
-__device__ __forceinline__ void item_box(const FusedParams& p, int node, float* bmin, float* bmax)
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        bmin[k] = p.tree.node_position_min[3 * node + k];
-        bmax[k] = p.tree.node_position_max[3 * node + k];
-    }
 }
 
 template <int C, int MODE, int H, int NH>
@@ -1175,14 +802,23 @@ static int prepare(const atdf_tree_t* tree, const atdf_field_t* field, const atd
 {
     if (!tree || !field || !mlp || !workspace || R < 0 || (R > 0 && (!origin || !dir)))
         return ATDF_ERR_INVALID_ARGUMENT;
-    if (field->dtype != ATDF_F32 || !field->leaf_slot) return ATDF_ERR_UNSUPPORTED;
-    var = find_variant(field, mlp);
-    if (!var) return ATDF_ERR_UNSUPPORTED;
+    if (!field->leaf_slot) return ATDF_ERR_INVALID_ARGUMENT;
+    var = nullptr;
+    if (field->dtype == ATDF_BF16) {
+        if (!tc_supported(field, mlp)) return ATDF_ERR_UNSUPPORTED;
+    } else if (field->dtype == ATDF_F32) {
+        var = find_variant(field, mlp);
+        if (!var) return ATDF_ERR_UNSUPPORTED;
+    } else {
+        return ATDF_ERR_UNSUPPORTED;
+    }
     for (int l = 0; l < mlp->num_layers; ++l)
         if (!mlp->weight[l] || !mlp->bias[l]) return ATDF_ERR_INVALID_ARGUMENT;
     int off = 0;
     for (int m = 0; m < 3; ++m) {
-        if (!field->plane[m] || !field->line[m] || ((uintptr_t)field->plane[m] & 15)) return ATDF_ERR_UNSUPPORTED;
+        if (!field->plane[m] || !field->line[m] || ((uintptr_t)field->plane[m] & 15) ||
+            ((uintptr_t)field->line[m] & 15))
+            return ATDF_ERR_UNSUPPORTED;
         p.plane_off[m] = off;
         off += field->plane_h[m] * field->plane_w[m] * field->channels;
     }
@@ -1261,7 +897,7 @@ int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, con
     ATDF_LAUNCH_CHECK();
     scan_exclusive_i32_kernel<<<1, 1024, 0, s>>>(w.item_offset, w.nslot + 2, nullptr);
     ATDF_LAUNCH_CHECK();
-    st = launch_persistent(var->fwd, var->smem(p.plane_off[3], false), p, s);
+    st = var ? launch_persistent(var->fwd, var->smem(p.plane_off[3], false), p, s) : launch_tc_forward(p, s);
     if (st != ATDF_OK) return st;
     if (num_rays > 0) {
         ray_reduce_kernel<<<(unsigned)div_up(num_rays, 256), 256, 0, s>>>(w, num_rays, image);
@@ -1304,7 +940,7 @@ int atdf_project_backward(const atdf_tree_t* tree, const atdf_field_t* field, co
         ATDF_CUDA_TRY(cudaMemsetAsync(grad_mlp->bias[l], 0, (size_t)mlp->dims[l + 1] * 4, s));
     }
     ATDF_CUDA_TRY(cudaMemsetAsync(p.ws.counters + 1, 0, 4, s));
-    return launch_persistent(var->bwd, var->smem(p.plane_off[3], true), p, s);
+    return var ? launch_persistent(var->bwd, var->smem(p.plane_off[3], true), p, s) : launch_tc_backward(p, s);
 }
 
 int atdf_project_node_error(const atdf_tree_t* tree, const float* ray_origin, const float* ray_direction,

@@ -1,0 +1,692 @@
+// Fused leaf-major projection with BF16 factor planes and the decoder on the
+// 5th-generation tensor cores (tcgen05, FP32 accumulation in TMEM), forward
+// and hand-written adjoint, for sm_100a. Shape: C = 16 channels ("add"),
+// decoder 16 -> 64 -> 64 -> 1 (the reference's FCBlock default with one
+// hidden layer of 64; hyperacorn/csrc/geometry/Modules.h:68-109).
+//
+// A CTA has two halves of 128 threads; each half owns a 128-sample tile, one
+// thread per sample (= one TMEM lane / accumulator row). Both halves share
+// the work item's planes (staged by TMA) and, in the backward, its shared
+// plane-gradient copy. Per tile:
+//   forward  X[128x16] -> D0 = X W0^T -> H0 = silu(D0 + b0)
+//            D1 = H0 W1^T -> silu(D1 + b1) . w2 + b2 -> softplus -> rho * w
+//   backward dz, dA1 = dz w2 silu'(A1);   dH0 = dA1 W1 -> dA0 = dH0 silu'(A0)
+//            dX = dA0 W0 -> scatter into the plane gradients
+//            [dW1 db1; dW0 db0] += [dA1 | dA0]^T [H0 | X | 1]   (one M=128 MMA,
+//            accumulated in TMEM across every tile of the CTA)
+// All MMA operands use the no-swizzle core-matrix layouts of tc.cuh, chosen
+// so one buffer serves several GEMMs: the buffer HB [128 x 96] (H0 | X | 1)
+// is the A operand of both forward layers (K-major views) and the B operand
+// of the weight-gradient MMA (MN-major); G [128 x 128] (dA1 | dA0) is the A
+// operand of dH0 and dX (K-major views) and of the weight-gradient MMA
+// (MN-major). W0 / W1 in [out][in] order are the K-major B of the forward
+// layers and, unchanged, the MN-major B of the backward ones.
+
+#include <cuda_bf16.h>
+
+#include "fused_common.cuh"
+#include "tc.cuh"
+
+namespace atdf {
+namespace tcf {
+
+constexpr int kC = 16;
+constexpr int kH = 64;
+constexpr int kRows = 128;          // samples per tile
+constexpr int kThreadsTC = 256;     // two halves
+constexpr int kHBCols = 96;         // H0 (64) | X (16) | ones | zero pad
+constexpr int kGCols = 128;         // dA1 (64) | dA0 (64)
+constexpr int kLineWinTC = 32;      // line-gradient window entries per line
+constexpr uint32_t kTmemFwd = 256;  // columns per CTA (2 CTAs per SM)
+constexpr uint32_t kTmemBwd = 512;
+
+__device__ __forceinline__ uint32_t hb_off(int s, int c) { return tc::mnmajor_off(c, s, kHBCols); }
+__device__ __forceinline__ uint32_t g_off(int s, int c) { return tc::mnmajor_off(c, s, kGCols); }
+__device__ __forceinline__ uint32_t w0_off(int n, int f) { return tc::kmajor_off(n, f, kC); }
+__device__ __forceinline__ uint32_t w1_off(int n, int k) { return tc::kmajor_off(n, k, kH); }
+
+struct TCSmem {
+    uint32_t planes, w0, w1, bias, hb[2], g[2], gplanes, gline, sw[2], sdi[2], sseg[2], segi, total;
+    __host__ __device__ TCSmem(int plane_elems, bool bwd)
+    {
+        auto al = [](uint32_t x) { return (x + 127u) & ~127u; };
+        uint32_t o = 0;
+        planes = o;
+        o = al(o + plane_elems * 2);
+        w0 = o;
+        o = al(o + kH * kC * 2);
+        w1 = o;
+        o = al(o + kH * kH * 2);
+        bias = o;  // b0[64] b1[64] w2[64] b2
+        o = al(o + (3 * kH + 4) * 4);
+        for (int h = 0; h < 2; ++h) {
+            hb[h] = o;
+            o = al(o + kRows * kHBCols * 2);
+        }
+        for (int h = 0; h < 2; ++h) {
+            g[h] = o;
+            if (bwd) o = al(o + kRows * kGCols * 2);
+        }
+        gplanes = o;
+        if (bwd) o = al(o + plane_elems * 4);
+        gline = o;
+        if (bwd) o = al(o + 3 * kLineWinTC * kC * 4);
+        for (int h = 0; h < 2; ++h) {
+            sw[h] = o;
+            o += kRows * 4;
+            sdi[h] = o;
+            o += kRows * 4;
+            sseg[h] = o;
+            o += kRows * 4;
+        }
+        o = al(o);
+        segi = o;
+        o = al(o + kSegTabArrays * (kSegItem + 4) * 4);
+        total = o;
+    }
+};
+
+// Shared plane-gradient copy: channel c of texel tau sits at position
+// c ^ (tau & 15), so the 32 samples of a warp, each at its own texel, hit
+// different banks for the same channel.
+__device__ __forceinline__ int gswz(int tau, int c) { return tau * kC + (c ^ (tau & (kC - 1))); }
+
+__device__ __forceinline__ void half_barrier(int h) { asm volatile("bar.sync %0, 128;" ::"r"(1 + h) : "memory"); }
+
+__device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t& phase, int32_t* err)
+{
+    const bool ok = mbar_wait(bar, phase);
+    phase ^= 1;
+    if (!ok) set_err(err, ATDF_DEVERR_TREE);
+    tc::fence_after_sync();
+    return ok;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void unpack_bf16x8(const uint4& u, float* f)
+{
+    const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 x = __bfloat1622float2(p[i]);
+        f[2 * i] = x.x;
+        f[2 * i + 1] = x.y;
+    }
+}
+
+// 8 FP32 values -> 8 BF16 at a 16-byte aligned shared address.
+__device__ __forceinline__ void store_bf16x8(unsigned char* dst, const float* v)
+{
+    uint4 u;
+    u.x = pack_bf16(v[0], v[1]);
+    u.y = pack_bf16(v[2], v[3]);
+    u.z = pack_bf16(v[4], v[5]);
+    u.w = pack_bf16(v[6], v[7]);
+    *reinterpret_cast<uint4*>(dst) = u;
+}
+
+__device__ __forceinline__ float silu(float x) { return x * sigmoidf_(x); }
+__device__ __forceinline__ float silu_grad(float x)
+{
+    const float s = sigmoidf_(x);
+    return s * (1.0f + x * (1.0f - s));
+}
+
+// VM feature of one sample (16 channels) from the BF16 planes in shared
+// memory and the BF16 lines in global memory.
+__device__ __forceinline__ void gather_features(const FusedParams& p, const unsigned char* sm, const SampleGeo& g,
+                                                float (&f)[kC], float (&mat)[3][kC], float (&vec)[3][kC])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
+        const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
+        const Corner1 l = corners1(g.lu[m], L);
+        const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
+        const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            float a[8], b[8], c[8], d[8], v0[8], v1[8];
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x0) * kC + 8 * half) * 2), a);
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x1) * kC + 8 * half) * 2), b);
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x0) * kC + 8 * half) * 2), c);
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x1) * kC + 8 * half) * 2), d);
+            unpack_bf16x8(__ldg(V + l.x0 * 2 + half), v0);
+            unpack_bf16x8(__ldg(V + l.x1 * 2 + half), v1);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int ch = 8 * half + i;
+                float acc = a[i] * k.w_nw;
+                acc = fmaf(b[i], k.w_ne, acc);
+                acc = fmaf(c[i], k.w_sw, acc);
+                acc = fmaf(d[i], k.w_se, acc);
+                mat[m][ch] = acc;
+                vec[m][ch] = fmaf(v0[i], l.w0, v1[i] * l.w1);
+            }
+        }
+    }
+#pragma unroll
+    for (int ch = 0; ch < kC; ++ch) f[ch] = fmaf(mat[0][ch], vec[0][ch], fmaf(mat[1][ch], vec[1][ch], mat[2][ch] * vec[2][ch]));
+}
+
+__device__ __forceinline__ void load_weights_tc(const FusedParams& p, unsigned char* sm, const TCSmem& L)
+{
+    const atdf_mlp_t& m = p.mlp;
+    for (int i = threadIdx.x; i < kH * kC; i += kThreadsTC) {
+        const int n = i / kC, f = i % kC;
+        *reinterpret_cast<__nv_bfloat16*>(sm + L.w0 + w0_off(n, f)) = __float2bfloat16_rn(m.weight[0][i]);
+    }
+    for (int i = threadIdx.x; i < kH * kH; i += kThreadsTC) {
+        const int n = i / kH, k = i % kH;
+        *reinterpret_cast<__nv_bfloat16*>(sm + L.w1 + w1_off(n, k)) = __float2bfloat16_rn(m.weight[1][i]);
+    }
+    float* bias = reinterpret_cast<float*>(sm + L.bias);
+    for (int i = threadIdx.x; i < kH; i += kThreadsTC) {
+        bias[i] = m.bias[0][i];
+        bias[kH + i] = m.bias[1][i];
+        bias[2 * kH + i] = m.weight[2][i];
+    }
+    if (threadIdx.x == 0) bias[3 * kH] = m.bias[2][0];
+}
+
+// Forward layer-0 / layer-1 MMAs of one half (issued by one thread).
+__device__ __forceinline__ void issue_l0(const unsigned char* sm, const TCSmem& L, int h, uint32_t d0)
+{
+    const uint64_t a = tc::smem_desc(tc::smem_addr(sm + L.hb[h] + (kH / 8) * 128), 128, 12 * 128);
+    const uint64_t b = tc::smem_desc(tc::smem_addr(sm + L.w0), 128, (kC / 8) * 128);
+    tc::mma_bf16(d0, a, b, tc::idesc_bf16(kRows, kH, 0, 0), 0);
+}
+
+__device__ __forceinline__ void issue_l1(const unsigned char* sm, const TCSmem& L, int h, uint32_t d1)
+{
+    const uint32_t abase = tc::smem_addr(sm + L.hb[h]), bbase = tc::smem_addr(sm + L.w1);
+#pragma unroll
+    for (int j = 0; j < kH / 16; ++j) {
+        const uint64_t a = tc::smem_desc(abase + j * 256, 128, 12 * 128);
+        const uint64_t b = tc::smem_desc(bbase + j * 256, 128, (kH / 8) * 128);
+        tc::mma_bf16(d1, a, b, tc::idesc_bf16(kRows, kH, 0, 0), j > 0);
+    }
+}
+
+// TMEM address of this thread's accumulator row at column col of a half.
+__device__ __forceinline__ uint32_t trow(uint32_t base, int col)
+{
+    const int warp = threadIdx.x >> 5;
+    return base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col;
+}
+
+// Forward sample features of tile row t into HB (X columns); returns validity.
+__device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned char* sm, const TCSmem& L,
+                                              const SegTab& tab, const ItemInfo& it, bool real, int h, int k,
+                                              int t, float& w, int& si, SampleGeo& g)
+{
+    const bool valid = k < it.total;
+    float f[kC];
+#pragma unroll
+    for (int i = 0; i < kC; ++i) f[i] = 0.0f;
+    w = 0.0f;
+    si = -1;
+    if (valid) {
+        const SampleState st = sample_state(p, tab, it.nseg, k);
+        w = st.w;
+        si = st.si;
+        if (real) {
+            g = sample_geo_fast(p, tab, st.si, st.pos);
+            float mat[3][kC], vec[3][kC];
+            gather_features(p, sm, g, f, mat, vec);
+        }
+    }
+    store_bf16x8(sm + L.hb[h] + hb_off(t, kH), f);
+    store_bf16x8(sm + L.hb[h] + hb_off(t, kH + 8), f + 8);
+    return valid;
+}
+
+// Layer-0 epilogue: H0 = silu(D0 + b0) into HB columns 0..63.
+__device__ __forceinline__ void epilogue_l0(unsigned char* sm, const TCSmem& L, int h, int t, uint32_t d0)
+{
+    const float* b0 = reinterpret_cast<const float*>(sm + L.bias);
+#pragma unroll
+    for (int j = 0; j < kH / 16; ++j) {
+        float v[16];
+        tc::ld_32x32b_x16(trow(d0, 16 * j), v);
+        tc::wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + b0[16 * j + i]);
+        store_bf16x8(sm + L.hb[h] + hb_off(t, 16 * j), v);
+        store_bf16x8(sm + L.hb[h] + hb_off(t, 16 * j + 8), v + 8);
+    }
+}
+
+__global__ void __launch_bounds__(kThreadsTC) tc_forward_kernel(FusedParams p)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ __align__(8) uint64_t bar_tma;
+    __shared__ __align__(8) uint64_t bar_mma[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_ctl[4];
+    const TCSmem L(p.plane_off[3], false);
+    const int tid = threadIdx.x, h = tid / kRows, t = tid % kRows;
+    if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemFwd);
+    if (tid == 0) {
+        mbar_init(&bar_tma, 1);
+        mbar_init(&bar_mma[0], 1);
+        mbar_init(&bar_mma[1], 1);
+    }
+    load_weights_tc(p, sm, L);
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = s_tmem + (uint32_t)(h * 128);
+    const uint32_t d0 = tbase, d1 = tbase + 64;
+    SegTab tab = seg_tab(reinterpret_cast<float*>(sm + L.segi));
+    const float* bias = reinterpret_cast<const float*>(sm + L.bias);
+    const float beta = p.mlp.softplus_beta;
+    const int lact = p.mlp.last_activation;
+    uint32_t tma_phase = 0, mma_phase = 0;
+    bool alive = true;
+    while (alive) {
+        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false);
+        if (it.slot < 0) break;
+        const bool real = it.slot < p.ws.nslot;
+        if (real) {
+            if (!mbar_wait(&bar_tma, tma_phase)) {
+                set_err(p.err, ATDF_DEVERR_TREE);
+                mbar_wait(&bar_tma, tma_phase);
+                alive = false;
+            }
+            tma_phase ^= 1;
+        }
+        alive = __syncthreads_and(alive);
+        for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
+            float w;
+            int si;
+            SampleGeo g;
+            const bool valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g);
+            tc::fence_smem_to_async();
+            tc::fence_before_sync();
+            half_barrier(h);
+            if (t == 0) {
+                tc::fence_after_sync();
+                issue_l0(sm, L, h, d0);
+                tc::commit(&bar_mma[h]);
+            }
+            alive = wait_mma(&bar_mma[h], mma_phase, p.err);
+            epilogue_l0(sm, L, h, t, d0);
+            tc::fence_smem_to_async();
+            tc::fence_before_sync();
+            half_barrier(h);
+            if (t == 0) {
+                tc::fence_after_sync();
+                issue_l1(sm, L, h, d1);
+                tc::commit(&bar_mma[h]);
+            }
+            alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
+            float z = bias[3 * kH];
+#pragma unroll
+            for (int j = 0; j < kH / 16; ++j) {
+                float v[16];
+                tc::ld_32x32b_x16(trow(d1, 16 * j), v);
+                tc::wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) z = fmaf(silu(v[i] + bias[kH + 16 * j + i]), bias[2 * kH + 16 * j + i], z);
+            }
+            if (valid) atomicAdd(&tab.acc[si], act_fwd(lact, z, beta) * w);
+            tc::fence_before_sync();
+            half_barrier(h);
+        }
+        alive = __syncthreads_and(alive);
+        if (tid < it.nseg) p.ws.seg_partial[tab.id[tid]] = tab.acc[tid];
+        __syncthreads();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid < 32) tc::tmem_dealloc(s_tmem, kTmemFwd);
+}
+
+__global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams p)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ __align__(8) uint64_t bar_tma;
+    __shared__ __align__(8) uint64_t bar_mma[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_ctl[4];
+    __shared__ int s_lo[3];
+    const TCSmem L(p.plane_off[3], true);
+    const int tid = threadIdx.x, h = tid / kRows, t = tid % kRows, lane = tid & 31;
+    if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemBwd);
+    if (tid == 0) {
+        mbar_init(&bar_tma, 1);
+        mbar_init(&bar_mma[0], 1);
+        mbar_init(&bar_mma[1], 1);
+    }
+    load_weights_tc(p, sm, L);
+    // ones column (80) and zero padding (81..95) of both HB buffers
+    for (int i = tid; i < 2 * kRows; i += kThreadsTC) {
+        const int hh = i / kRows, s = i % kRows;
+        float v[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        store_bf16x8(sm + L.hb[hh] + hb_off(s, 80), v);
+        v[0] = 0.f;
+        store_bf16x8(sm + L.hb[hh] + hb_off(s, 88), v);
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = s_tmem + (uint32_t)(h * 256);
+    const uint32_t d0 = tbase, d1 = tbase + 64, dacc = tbase + 128;
+    SegTab tab = seg_tab(reinterpret_cast<float*>(sm + L.segi));
+    const float* bias = reinterpret_cast<const float*>(sm + L.bias);
+    const float beta = p.mlp.softplus_beta;
+    const int lact = p.mlp.last_activation;
+    const int C = kC;
+    const int plane_elems = p.plane_off[3];
+    float* gpl = reinterpret_cast<float*>(sm + L.gplanes);
+    float* gln = reinterpret_cast<float*>(sm + L.gline);
+    uint32_t tma_phase = 0, mma_phase = 0;
+    bool alive = true, had_tile = false;
+    float gw2a = 0.f, gw2b = 0.f, gb2 = 0.f;  // lane owns last-layer columns 2*lane, 2*lane+1
+    while (alive) {
+        const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
+        if (it.slot < 0) break;
+        const bool real = it.slot < p.ws.nslot;
+        if (real) {
+            for (int i = tid * 4; i < plane_elems; i += kThreadsTC * 4)
+                *reinterpret_cast<float4*>(gpl + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsTC) gln[i] = 0.0f;
+            if (tid < 3) {
+                float bmin[3], bmax[3];
+                item_box(p, tab.node[0], bmin, bmax);
+                const int Ln = p.field.line_len[tid];
+                int lo = 0;
+                if (Ln > kLineWinTC) {
+                    const float u = tid == 0 ? roi_coord(bmin[0], p.field.roi_min[0], p.field.roi_max[0])
+                                             : (tid == 2 ? bmin[2] : -1.0f);
+                    lo = (int)floorf(((u + 1.0f) * 0.5f) * (float)(Ln - 1)) - 2;
+                    lo = max(0, min(lo, Ln - kLineWinTC));
+                }
+                s_lo[tid] = lo;
+            }
+            if (!mbar_wait(&bar_tma, tma_phase)) {
+                set_err(p.err, ATDF_DEVERR_TREE);
+                mbar_wait(&bar_tma, tma_phase);
+                alive = false;
+            }
+            tma_phase ^= 1;
+        }
+        alive = __syncthreads_and(alive);
+        for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
+            float w;
+            int si;
+            SampleGeo g;
+            const bool valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g);
+            const float dIw = valid ? tab.acc[si] * w : 0.0f;
+            tc::fence_smem_to_async();
+            tc::fence_before_sync();
+            half_barrier(h);
+            if (t == 0) {
+                tc::fence_after_sync();
+                issue_l0(sm, L, h, d0);
+                tc::commit(&bar_mma[h]);
+            }
+            alive = wait_mma(&bar_mma[h], mma_phase, p.err);
+            epilogue_l0(sm, L, h, t, d0);
+            tc::fence_smem_to_async();
+            tc::fence_before_sync();
+            half_barrier(h);
+            if (t == 0) {
+                tc::fence_after_sync();
+                issue_l1(sm, L, h, d1);
+                tc::commit(&bar_mma[h]);
+            }
+            alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
+            // last layer: z, dz; dA1 = dz w2 silu'(A1) into G columns 0..63
+            float a1[kH];
+#pragma unroll
+            for (int j = 0; j < kH / 16; ++j) {
+                float v[16];
+                tc::ld_32x32b_x16(trow(d1, 16 * j), v);
+                tc::wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bias[kH + 16 * j + i];
+            }
+            float z = bias[3 * kH];
+#pragma unroll
+            for (int k = 0; k < kH; ++k) z = fmaf(silu(a1[k]), bias[2 * kH + k], z);
+            const float dz = dIw * act_grad(lact, z, beta);
+            {
+                float da[16];
+#pragma unroll
+                for (int j = 0; j < kH / 16; ++j) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int k = 16 * j + i;
+                        da[i] = dz * bias[2 * kH + k] * silu_grad(a1[k]);
+                    }
+                    store_bf16x8(sm + L.g[h] + g_off(t, 16 * j), da);
+                    store_bf16x8(sm + L.g[h] + g_off(t, 16 * j + 8), da + 8);
+                }
+            }
+            // last-layer weight gradient: reduce dz * silu(a1[k]) over the warp's
+            // 32 rows, halving the value set each round; lane ends with 2 columns
+            {
+#pragma unroll
+                for (int k = 0; k < kH; ++k) a1[k] = dz * silu(a1[k]);
+                int n = kH;
+#pragma unroll
+                for (int off = 16; off >= 1; off >>= 1) {
+                    const bool upper = (lane & off) != 0;
+                    n >>= 1;
+#pragma unroll
+                    for (int k = 0; k < kH / 2; ++k) {
+                        if (k < n) {
+                            const float send = upper ? a1[k] : a1[k + n];
+                            const float keep = upper ? a1[k + n] : a1[k];
+                            a1[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+                        }
+                    }
+                }
+                gw2a += a1[0];
+                gw2b += a1[1];
+                float s = dz;
+#pragma unroll
+                for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+                if (lane == 0) gb2 += s;
+            }
+            tc::fence_smem_to_async();
+            tc::fence_before_sync();
+            half_barrier(h);
+            if (t == 0) {  // dH0 = dA1 W1 into the D1 columns
+                tc::fence_after_sync();
+                const uint32_t abase = tc::smem_addr(sm + L.g[h]), bbase = tc::smem_addr(sm + L.w1);
+#pragma unroll
+                for (int j = 0; j < kH / 16; ++j) {
+                    const uint64_t a = tc::smem_desc(abase + j * 256, 128, (kGCols / 8) * 128);
+                    const uint64_t b = tc::smem_desc(bbase + j * 2 * (kH / 8) * 128, (kH / 8) * 128, 128);
+                    tc::mma_bf16(d1, a, b, tc::idesc_bf16(kRows, kH, 0, 1), j > 0);
+                }
+                tc::commit(&bar_mma[h]);
+            }
+            alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
+            // dA0 = dH0 silu'(A0) into G columns 64..127 (A0 = D0 + b0)
+#pragma unroll
+            for (int j = 0; j < kH / 16; ++j) {
+                float gv[16], av[16], da[16];
+                tc::ld_32x32b_x16(trow(d1, 16 * j), gv);
+                tc::ld_32x32b_x16(trow(d0, 16 * j), av);
+                tc::wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bias[16 * j + i]);
+                store_bf16x8(sm + L.g[h] + g_off(t, kH + 16 * j), da);
+                store_bf16x8(sm + L.g[h] + g_off(t, kH + 16 * j + 8), da + 8);
+            }
+            tc::fence_smem_to_async();
+            tc::fence_before_sync();
+            half_barrier(h);
+            if (t == 0) {
+                tc::fence_after_sync();
+                // dX = dA0 W0 into the D0 columns 0..15
+                const uint32_t abase = tc::smem_addr(sm + L.g[h] + (kH / 8) * 128), bbase = tc::smem_addr(sm + L.w0);
+#pragma unroll
+                for (int j = 0; j < kH / 16; ++j) {
+                    const uint64_t a = tc::smem_desc(abase + j * 256, 128, (kGCols / 8) * 128);
+                    const uint64_t b = tc::smem_desc(bbase + j * 2 * (kC / 8) * 128, (kC / 8) * 128, 128);
+                    tc::mma_bf16(d0, a, b, tc::idesc_bf16(kRows, kC, 0, 1), j > 0);
+                }
+                // [dW1 db1; dW0 db0] += [dA1 | dA0]^T [H0 | X | 1]
+                const uint32_t gbase = tc::smem_addr(sm + L.g[h]), hbase = tc::smem_addr(sm + L.hb[h]);
+#pragma unroll
+                for (int j = 0; j < kRows / 16; ++j) {
+                    const uint64_t a = tc::smem_desc(gbase + j * 2 * (kGCols / 8) * 128, (kGCols / 8) * 128, 128);
+                    const uint64_t b = tc::smem_desc(hbase + j * 2 * (kHBCols / 8) * 128, (kHBCols / 8) * 128, 128);
+                    tc::mma_bf16(dacc, a, b, tc::idesc_bf16(kRows, kHBCols, 1, 1), (had_tile || j > 0) ? 1u : 0u);
+                }
+                tc::commit(&bar_mma[h]);
+            }
+            had_tile = true;
+            alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
+            // scatter dX into the shared plane gradient and the line windows
+            {
+                float dx[16];
+                tc::ld_32x32b_x16(trow(d0, 0), dx);
+                tc::wait_ld();
+                if (valid && real) {
+                    float f[kC], mat[3][kC], vec[3][kC];
+                    gather_features(p, sm, g, f, mat, vec);
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], Ln = p.field.line_len[m];
+                        const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
+                        const Corner1 l = corners1(g.lu[m], Ln);
+                        float* GP = gpl + p.plane_off[m];
+                        const int lo = s_lo[m];
+                        const int i0 = l.x0 - lo, i1 = l.x1 - lo;
+#pragma unroll
+                        for (int c = 0; c < kC; ++c) {
+                            const float gm = dx[c] * vec[m][c], gv = dx[c] * mat[m][c];
+                            atomicAdd(&GP[gswz(kc.y0 * Wm + kc.x0, c)], kc.w_nw * gm);
+                            atomicAdd(&GP[gswz(kc.y0 * Wm + kc.x1, c)], kc.w_ne * gm);
+                            atomicAdd(&GP[gswz(kc.y1 * Wm + kc.x0, c)], kc.w_sw * gm);
+                            atomicAdd(&GP[gswz(kc.y1 * Wm + kc.x1, c)], kc.w_se * gm);
+                            if (i0 >= 0 && i0 < kLineWinTC)
+                                atomicAdd(&gln[(m * kLineWinTC + i0) * C + c], l.w0 * gv);
+                            else
+                                atomicAdd(&p.gfield.line[m][l.x0 * C + c], l.w0 * gv);
+                            if (i1 >= 0 && i1 < kLineWinTC)
+                                atomicAdd(&gln[(m * kLineWinTC + i1) * C + c], l.w1 * gv);
+                            else
+                                atomicAdd(&p.gfield.line[m][l.x1 * C + c], l.w1 * gv);
+                        }
+                    }
+                }
+            }
+            tc::fence_before_sync();
+            half_barrier(h);
+        }
+        alive = __syncthreads_and(alive);
+        if (real) {
+            for (int m = 0; m < 3; ++m) {
+                const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
+                float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
+                const float* src = gpl + p.plane_off[m];
+                for (int i = tid * 4; i < pf; i += kThreadsTC * 4) {
+                    // un-swizzle: quad q of texel tau is stored at quad q ^ (m >> 2),
+                    // element e of it at position e ^ (m & 3), with m = tau & 15
+                    const int tau = i / kC, q = (i % kC) / 4, msk = tau & (kC - 1);
+                    const float4 v = *reinterpret_cast<const float4*>(src + tau * kC + 4 * (q ^ (msk >> 2)));
+                    const float a[4] = {v.x, v.y, v.z, v.w};
+                    const int x = msk & 3;
+                    atomicAdd(reinterpret_cast<float4*>(dst + i), make_float4(a[0 ^ x], a[1 ^ x], a[2 ^ x], a[3 ^ x]));
+                }
+                const int Ln = p.field.line_len[m];
+                const int lo = s_lo[m];
+                for (int i = tid; i < kLineWinTC * C; i += kThreadsTC) {
+                    const int e = lo + i / C;
+                    const float v = gln[m * kLineWinTC * C + i];
+                    if (e < Ln && v != 0.0f) atomicAdd(&p.gfield.line[m][e * C + (i % C)], v);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // decoder gradients: the TMEM accumulator rows of this half
+    if (had_tile) {
+        tc::fence_after_sync();
+#pragma unroll
+        for (int j = 0; j < kHBCols / 16; ++j) {
+            float v[16];
+            tc::ld_32x32b_x16(trow(dacc, 16 * j), v);
+            tc::wait_ld();
+            if (t < kH) {  // rows 0..63: dW1 (cols 0..63), db1 (col 80)
+                if (j < 4)
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) atomicAdd(&p.gmlp.weight[1][t * kH + 16 * j + i], v[i]);
+                if (j == 5) atomicAdd(&p.gmlp.bias[1][t], v[0]);
+            } else {  // rows 64..127: dW0 (cols 64..79), db0 (col 80)
+                const int n = t - kH;
+                if (j == 4)
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) atomicAdd(&p.gmlp.weight[0][n * kC + i], v[i]);
+                if (j == 5) atomicAdd(&p.gmlp.bias[0][n], v[0]);
+            }
+        }
+    }
+    // last layer: lane l's two columns are given by the halving order above
+    {
+        int colbits = 0;
+        for (int off = 16, b = 0; off >= 1; off >>= 1, ++b)
+            if (lane & off) colbits |= (kH >> (b + 1));
+        atomicAdd(&p.gmlp.weight[2][colbits], gw2a);
+        atomicAdd(&p.gmlp.weight[2][colbits + 1], gw2b);
+        if (lane == 0) atomicAdd(&p.gmlp.bias[2][0], gb2);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid < 32) tc::tmem_dealloc(s_tmem, kTmemBwd);
+}
+
+}  // namespace tcf
+
+bool tc_supported(const atdf_field_t* f, const atdf_mlp_t* m)
+{
+    return f->dtype == ATDF_BF16 && f->channels == tcf::kC && f->mode == 0 && m->num_layers == 3 &&
+           m->dims[0] == tcf::kC && m->dims[1] == tcf::kH && m->dims[2] == tcf::kH && m->dims[3] == 1 &&
+           m->hidden_activation == ATDF_ACT_SILU;
+}
+
+static int max_optin()
+{
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cudaStream_t st)
+{
+    const int smem = (int)tcf::TCSmem(p.plane_off[3], bwd).total;
+    if (smem > max_optin()) return ATDF_ERR_UNSUPPORTED;
+    ATDF_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int dev = 0, sms = 0, per = 0;
+    ATDF_CUDA_TRY(cudaGetDevice(&dev));
+    ATDF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    ATDF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, tcf::kThreadsTC, smem));
+    if (per < 1) return ATDF_ERR_UNSUPPORTED;
+    // TMEM: 256 columns per forward CTA, 512 per backward CTA (512 per SM)
+    per = std::min(per, bwd ? 1 : 2);
+    fn<<<sms * per, tcf::kThreadsTC, smem, st>>>(p);
+    ATDF_LAUNCH_CHECK();
+    return ATDF_OK;
+}
+
+int launch_tc_forward(const FusedParams& p, cudaStream_t st) { return launch_tc(tcf::tc_forward_kernel, false, p, st); }
+int launch_tc_backward(const FusedParams& p, cudaStream_t st) { return launch_tc(tcf::tc_backward_kernel, true, p, st); }
+
+}  // namespace atdf

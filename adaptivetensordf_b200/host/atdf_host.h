@@ -106,6 +106,13 @@ struct GeometryTensorQO {
     std::vector<double> roi_min{-1, -1, -1}, roi_max{1, 1, 1};
     std::string tensor_op = "add";
     Decoder decoder;
+    // "fp32": the fused path reads the FP32 planes / lines. "bf16": it reads
+    // BF16 working copies (planes_bf16 / lines_bf16, refreshed from the FP32
+    // parameters by RefreshLowPrecision) and runs the decoder on the tensor
+    // cores; gradients still flow to the FP32 parameters.
+    std::string precision = "fp32";
+    std::vector<torch::Tensor> planes_bf16, lines_bf16;
+    void RefreshLowPrecision();
 
     atdf_field_t view() const;
     torch::Tensor SampleVolumeIndirect_feature(HyperTreeBase& tree, torch::Tensor global_coordinate,

@@ -99,6 +99,10 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def_readwrite("roi_min", &GeometryTensorQO::roi_min)
         .def_readwrite("roi_max", &GeometryTensorQO::roi_max)
         .def_readwrite("tensor_op", &GeometryTensorQO::tensor_op)
+        .def_readwrite("precision", &GeometryTensorQO::precision)
+        .def_readonly("planes_bf16", &GeometryTensorQO::planes_bf16)
+        .def_readonly("lines_bf16", &GeometryTensorQO::lines_bf16)
+        .def("RefreshLowPrecision", &GeometryTensorQO::RefreshLowPrecision)
         .def_property(
             "decoder_weight", [](GeometryTensorQO& g) { return g.decoder.weight; },
             [](GeometryTensorQO& g, std::vector<torch::Tensor> v) { g.decoder.weight = v; })

@@ -389,6 +389,58 @@ static atdf_field_t field_view(const GeometryTensorQO& g, const std::vector<Tens
     return f;
 }
 
+void GeometryTensorQO::RefreshLowPrecision()
+{
+    torch::NoGradGuard ng;
+    const bool fresh = planes_bf16.size() != 3;
+    if (fresh) {
+        planes_bf16.clear();
+        lines_bf16.clear();
+    }
+    for (int m = 0; m < 3; ++m) {
+        if (fresh) {
+            planes_bf16.push_back(torch::empty(planes[m].sizes(), planes[m].options().dtype(torch::kBFloat16))
+                                      .contiguous(torch::MemoryFormat::ChannelsLast));
+            lines_bf16.push_back(torch::empty(lines[m].sizes(), lines[m].options().dtype(torch::kBFloat16))
+                                     .contiguous(torch::MemoryFormat::ChannelsLast));
+        }
+        planes_bf16[m].copy_(planes[m]);
+        lines_bf16[m].copy_(lines[m]);
+    }
+}
+
+// Field view over the BF16 working copies (the shapes are the FP32 ones).
+static atdf_field_t field_view_bf16(const GeometryTensorQO& g, const std::vector<Tensor>& planes32)
+{
+    TORCH_CHECK(g.planes_bf16.size() == 3 && g.lines_bf16.size() == 3,
+                "precision bf16: call RefreshLowPrecision() after creating or updating the parameters");
+    atdf_field_t f;
+    std::memset(&f, 0, sizeof(f));
+    f.channels = (int32_t)planes32[0].size(1);
+    f.mode = g.tensor_op == "cat" ? 1 : 0;
+    f.dtype = ATDF_BF16;
+    for (int m = 0; m < 3; ++m) {
+        const auto& p = g.planes_bf16[m];
+        const auto& l = g.lines_bf16[m];
+        TORCH_CHECK(p.sizes() == planes32[m].sizes() && p.is_contiguous(torch::MemoryFormat::ChannelsLast) &&
+                        l.is_contiguous(torch::MemoryFormat::ChannelsLast) && p.scalar_type() == torch::kBFloat16,
+                    "BF16 working copies out of date: call RefreshLowPrecision()");
+        f.plane[m] = p.data_ptr();
+        f.plane_h[m] = (int32_t)p.size(2);
+        f.plane_w[m] = (int32_t)p.size(3);
+        f.line[m] = l.data_ptr();
+        f.line_len[m] = (int32_t)l.size(2);
+        f.roi_min[m] = (float)g.roi_min[m];
+        f.roi_max[m] = (float)g.roi_max[m];
+    }
+    f.leaf_slot = g.leaf_slot.data_ptr<int64_t>();
+    f.num_slots = planes32[0].size(0);
+    return f;
+}
+
+static atdf_field_t fused_field_view(const GeometryTensorQO& g, const std::vector<Tensor>& planes,
+                                     const std::vector<Tensor>& lines);
+
 atdf_field_t GeometryTensorQO::view() const
 {
     std::vector<Tensor> p, l;
@@ -484,6 +536,14 @@ Tensor GeometryTensorQO::ComputeImage(HyperTreeBase& tree, const SampleList& sam
     return IntegrateSamplesXRay(out, samples.weight.unsqueeze(1), samples.ray_index, num_channels, num_pixels);
 }
 
+static atdf_field_t fused_field_view(const GeometryTensorQO& g, const std::vector<Tensor>& planes,
+                                     const std::vector<Tensor>& lines)
+{
+    if (g.precision == "bf16") return field_view_bf16(g, planes);
+    TORCH_CHECK(g.precision == "fp32", "precision must be fp32 or bf16");
+    return field_view(g, planes, lines);
+}
+
 // ---------------------------------------------------------------------------
 // Fused projection with the hand-written adjoint
 // ---------------------------------------------------------------------------
@@ -501,7 +561,7 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
     {
         auto* a = reinterpret_cast<ProjectArgs*>(args_ptr);
         std::vector<Tensor> P{p0, p1, p2}, L{l0, l1, l2};
-        auto f = field_view(*a->geo, P, L);
+        auto f = fused_field_view(*a->geo, P, L);
         auto dims = layer_dims(a->geo->decoder);
         const int act = activation_id(a->geo->decoder.activation), last = activation_id(a->geo->decoder.last_activation);
         const float beta = (float)a->geo->decoder.softplus_beta;
@@ -536,7 +596,7 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
         auto* tree = reinterpret_cast<HyperTreeBase*>(ctx->saved_data["tree"].toInt());
         std::vector<Tensor> P{s[2], s[3], s[4]}, L{s[5], s[6], s[7]};
         auto flat = s[8];
-        auto f = field_view(*geo, P, L);
+        auto f = fused_field_view(*geo, P, L);
         auto dims = layer_dims(geo->decoder);
         auto m = mlp_view(dims, flat.data_ptr<float>(), activation_id(geo->decoder.activation),
                           activation_id(geo->decoder.last_activation), (float)geo->decoder.softplus_beta);
@@ -583,7 +643,12 @@ std::tuple<Tensor, Tensor, Tensor> GeometryTensorQO::ProjectNodeError(HyperTreeB
 {
     torch::NoGradGuard ng;
     ATDF_CHECK_CUDA(rays.origin);
-    auto f = view();
+    std::vector<Tensor> P, L;
+    for (int m = 0; m < 3; ++m) {
+        P.push_back(channels_last(planes[m]));
+        L.push_back(channels_last(lines[m]));
+    }
+    auto f = fused_field_view(*this, P, L);
     auto dims = layer_dims(decoder);
     auto flat = flat_params(decoder);
     auto m = mlp_view(dims, flat.data_ptr<float>(), activation_id(decoder.activation),
