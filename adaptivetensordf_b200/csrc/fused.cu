@@ -227,7 +227,7 @@ struct Smem {
         sseg = o;
         o += kT;
         segi = o;
-        o += kSegTabArrays * (kSegItem + 4);
+        o += kSegTabFloats;
         total = o;
     }
 };
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
             float w = 0.0f;
             int si = -1;
             if (valid) {
-                const SampleState st = sample_state(p, tab, it.nseg, k);
+                const SampleState st = sample_state(p, tab, it, k);
                 w = st.w;
                 si = st.si;
                 if (real) {
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
             float w = 0.0f, dIw = 0.0f;
             SampleGeo g;
             if (valid) {
-                const SampleState st = sample_state(p, tab, it.nseg, k);
+                const SampleState st = sample_state(p, tab, it, k);
                 w = st.w;
                 dIw = __fmul_rn(tab.acc[st.si], st.w);
                 if (real) {

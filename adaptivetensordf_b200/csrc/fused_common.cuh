@@ -13,6 +13,7 @@ namespace atdf {
 constexpr int kSegItem = 64;          // segments per work item
 constexpr int kLineWin = 64;          // line-gradient window entries per line
 constexpr int kSegTabArrays = 18;     // arrays of the per-item segment table
+constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4);  // floats of the per-item table
 
 // ---------------------------------------------------------------------------
 // workspace
@@ -204,6 +205,13 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
 
 // Takes the next work item; fills the segment table; issues the plane TMA.
 // Returns the item's slot, or -1 when the queue is empty.
+// A work item's samples are visited in the order k -> k * 104729 mod total
+// (a permutation: the prime exceeds any item's sample count). Consecutive
+// samples, which share a warp, then come from different rays and depths in
+// the leaf and touch different texels, so their shared-memory atomics do not
+// collide the way the samples along one ray would.
+constexpr int kSamplePermPrime = 104729;
+
 struct ItemInfo {
     int64_t slot;
     int nseg;
@@ -333,11 +341,13 @@ __device__ __forceinline__ float sample_t_step(float tmin, float step, int j, fl
     return __fadd_rn(__fmul_rn(t1, oma), __fmul_rn(t2, a));
 }
 
-__device__ __forceinline__ SampleState sample_state(const FusedParams& p, const SegTab& tab, int nseg, int k)
+__device__ __forceinline__ SampleState sample_state(const FusedParams& p, const SegTab& tab, const ItemInfo& it,
+                                                    int k)
 {
     SampleState s;
-    s.si = find_seg(tab, nseg, k);
-    const int j = k - tab.start[s.si];
+    const int kk = it.total < kSamplePermPrime ? (int)(((long long)k * kSamplePermPrime) % it.total) : k;
+    s.si = find_seg(tab, it.nseg, kk);
+    const int j = kk - tab.start[s.si];
     const int n = tab.n[s.si];
     const int r = tab.ray[s.si];
     s.node = tab.node[s.si];

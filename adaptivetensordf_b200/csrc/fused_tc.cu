@@ -81,15 +81,10 @@ struct TCSmem {
         }
         o = al(o);
         segi = o;
-        o = al(o + kSegTabArrays * (kSegItem + 4) * 4);
+        o = al(o + kSegTabFloats * 4);
         total = o;
     }
 };
-
-// Shared plane-gradient copy: channel c of texel tau sits at position
-// c ^ (tau & 15), so the 32 samples of a warp, each at its own texel, hit
-// different banks for the same channel.
-__device__ __forceinline__ int gswz(int tau, int c) { return tau * kC + (c ^ (tau & (kC - 1))); }
 
 __device__ __forceinline__ void half_barrier(int h) { asm volatile("bar.sync %0, 128;" ::"r"(1 + h) : "memory"); }
 
@@ -130,11 +125,33 @@ __device__ __forceinline__ void store_bf16x8(unsigned char* dst, const float* v)
     *reinterpret_cast<uint4*>(dst) = u;
 }
 
-__device__ __forceinline__ float silu(float x) { return x * sigmoidf_(x); }
+// Logistic function from the hardware tanh approximation (one MUFU op,
+// ~2^-11 relative error, below the BF16 rounding of the activations).
+__device__ __forceinline__ float sigmoid_tanh(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(0.5f * x));
+    return fmaf(0.5f, y, 0.5f);
+}
+__device__ __forceinline__ float silu(float x) { return x * sigmoid_tanh(x); }
 __device__ __forceinline__ float silu_grad(float x)
 {
-    const float s = sigmoidf_(x);
+    const float s = sigmoid_tanh(x);
     return s * (1.0f + x * (1.0f - s));
+}
+
+// 16 consecutive floats of the bias block (16-byte aligned) into registers.
+__device__ __forceinline__ void ld16(const float* src, float (&v)[16])
+{
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 x = s4[q];
+        v[4 * q] = x.x;
+        v[4 * q + 1] = x.y;
+        v[4 * q + 2] = x.z;
+        v[4 * q + 3] = x.w;
+    }
 }
 
 // VM feature of one sample (16 channels) from the BF16 planes in shared
@@ -172,6 +189,38 @@ __device__ __forceinline__ void gather_features(const FusedParams& p, const unsi
     }
 #pragma unroll
     for (int ch = 0; ch < kC; ++ch) f[ch] = fmaf(mat[0][ch], vec[0][ch], fmaf(mat[1][ch], vec[1][ch], mat[2][ch] * vec[2][ch]));
+}
+
+
+// Bilinear plane value and linear line value of plane / line m for the 16
+// channels of one sample (the backward's recomputation of its gathers).
+__device__ __forceinline__ void gather_plane(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
+                                             float (&mat)[kC], float (&vec)[kC])
+{
+    const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
+    const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
+    const Corner1 l = corners1(g.lu[m], L);
+    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
+    const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        float a[8], b[8], c[8], d[8], v0[8], v1[8];
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x0) * kC + 8 * half) * 2), a);
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x1) * kC + 8 * half) * 2), b);
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x0) * kC + 8 * half) * 2), c);
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x1) * kC + 8 * half) * 2), d);
+        unpack_bf16x8(__ldg(V + l.x0 * 2 + half), v0);
+        unpack_bf16x8(__ldg(V + l.x1 * 2 + half), v1);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float acc = a[i] * k.w_nw;
+            acc = fmaf(b[i], k.w_ne, acc);
+            acc = fmaf(c[i], k.w_sw, acc);
+            acc = fmaf(d[i], k.w_se, acc);
+            mat[8 * half + i] = acc;
+            vec[8 * half + i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
+        }
+    }
 }
 
 __device__ __forceinline__ void load_weights_tc(const FusedParams& p, unsigned char* sm, const TCSmem& L)
@@ -232,7 +281,7 @@ __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned cha
     w = 0.0f;
     si = -1;
     if (valid) {
-        const SampleState st = sample_state(p, tab, it.nseg, k);
+        const SampleState st = sample_state(p, tab, it, k);
         w = st.w;
         si = st.si;
         if (real) {
@@ -252,11 +301,12 @@ __device__ __forceinline__ void epilogue_l0(unsigned char* sm, const TCSmem& L, 
     const float* b0 = reinterpret_cast<const float*>(sm + L.bias);
 #pragma unroll
     for (int j = 0; j < kH / 16; ++j) {
-        float v[16];
+        float v[16], bb[16];
         tc::ld_32x32b_x16(trow(d0, 16 * j), v);
+        ld16(b0 + 16 * j, bb);
         tc::wait_ld();
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + b0[16 * j + i]);
+        for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + bb[i]);
         store_bf16x8(sm + L.hb[h] + hb_off(t, 16 * j), v);
         store_bf16x8(sm + L.hb[h] + hb_off(t, 16 * j + 8), v + 8);
     }
@@ -330,11 +380,13 @@ __global__ void __launch_bounds__(kThreadsTC) tc_forward_kernel(FusedParams p)
             float z = bias[3 * kH];
 #pragma unroll
             for (int j = 0; j < kH / 16; ++j) {
-                float v[16];
+                float v[16], bb[16], ww[16];
                 tc::ld_32x32b_x16(trow(d1, 16 * j), v);
+                ld16(bias + kH + 16 * j, bb);
+                ld16(bias + 2 * kH + 16 * j, ww);
                 tc::wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) z = fmaf(silu(v[i] + bias[kH + 16 * j + i]), bias[2 * kH + 16 * j + i], z);
+                for (int i = 0; i < 16; ++i) z = fmaf(silu(v[i] + bb[i]), ww[i], z);
             }
             if (valid) atomicAdd(&tab.acc[si], act_fwd(lact, z, beta) * w);
             tc::fence_before_sync();
@@ -422,10 +474,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
         }
         alive = __syncthreads_and(alive);
         for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
+            bool valid = false;
+            SampleGeo g;
             float w;
             int si;
-            SampleGeo g;
-            const bool valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g);
+            valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g);
             const float dIw = valid ? tab.acc[si] * w : 0.0f;
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -450,25 +503,30 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
             float a1[kH];
 #pragma unroll
             for (int j = 0; j < kH / 16; ++j) {
-                float v[16];
+                float v[16], bb[16];
                 tc::ld_32x32b_x16(trow(d1, 16 * j), v);
+                ld16(bias + kH + 16 * j, bb);
                 tc::wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bias[kH + 16 * j + i];
+                for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bb[i];
             }
             float z = bias[3 * kH];
 #pragma unroll
-            for (int k = 0; k < kH; ++k) z = fmaf(silu(a1[k]), bias[2 * kH + k], z);
+            for (int j = 0; j < kH / 16; ++j) {
+                float ww[16];
+                ld16(bias + 2 * kH + 16 * j, ww);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) z = fmaf(silu(a1[16 * j + i]), ww[i], z);
+            }
             const float dz = dIw * act_grad(lact, z, beta);
             {
                 float da[16];
 #pragma unroll
                 for (int j = 0; j < kH / 16; ++j) {
+                    float ww[16];
+                    ld16(bias + 2 * kH + 16 * j, ww);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const int k = 16 * j + i;
-                        da[i] = dz * bias[2 * kH + k] * silu_grad(a1[k]);
-                    }
+                    for (int i = 0; i < 16; ++i) da[i] = dz * ww[i] * silu_grad(a1[16 * j + i]);
                     store_bf16x8(sm + L.g[h] + g_off(t, 16 * j), da);
                     store_bf16x8(sm + L.g[h] + g_off(t, 16 * j + 8), da + 8);
                 }
@@ -517,12 +575,13 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
             // dA0 = dH0 silu'(A0) into G columns 64..127 (A0 = D0 + b0)
 #pragma unroll
             for (int j = 0; j < kH / 16; ++j) {
-                float gv[16], av[16], da[16];
+                float gv[16], av[16], da[16], bb[16];
                 tc::ld_32x32b_x16(trow(d1, 16 * j), gv);
                 tc::ld_32x32b_x16(trow(d0, 16 * j), av);
+                ld16(bias + 16 * j, bb);
                 tc::wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bias[16 * j + i]);
+                for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bb[i]);
                 store_bf16x8(sm + L.g[h] + g_off(t, kH + 16 * j), da);
                 store_bf16x8(sm + L.g[h] + g_off(t, kH + 16 * j + 8), da + 8);
             }
@@ -551,37 +610,63 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
             }
             had_tile = true;
             alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
-            // scatter dX into the shared plane gradient and the line windows
+            // scatter dX into the shared plane gradient and the line windows.
+            // Shared-memory float atomics are fast when the 32 lanes of a warp
+            // hit 32 different banks and slow when they collide: each lane walks
+            // the 16 channels starting at its own lane index, reading the values
+            // back from its row of the (now free) G buffer.
             {
                 float dx[16];
                 tc::ld_32x32b_x16(trow(d0, 0), dx);
                 tc::wait_ld();
                 if (valid && real) {
-                    float f[kC], mat[3][kC], vec[3][kC];
-                    gather_features(p, sm, g, f, mat, vec);
-#pragma unroll
+                    float* mine = reinterpret_cast<float*>(sm + L.g[h]) + t * (kC + 4);
+#pragma unroll 1
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], Ln = p.field.line_len[m];
+                        float mat[kC], vec[kC];
+                        gather_plane(p, sm, g, m, mat, vec);
                         const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
                         const Corner1 l = corners1(g.lu[m], Ln);
+#pragma unroll
+                        for (int q = 0; q < kC / 4; ++q)
+                            *reinterpret_cast<float4*>(mine + 4 * q) =
+                                make_float4(dx[4 * q] * vec[4 * q], dx[4 * q + 1] * vec[4 * q + 1],
+                                            dx[4 * q + 2] * vec[4 * q + 2], dx[4 * q + 3] * vec[4 * q + 3]);
                         float* GP = gpl + p.plane_off[m];
+                        const int t00 = (kc.y0 * Wm + kc.x0) * C, t01 = (kc.y0 * Wm + kc.x1) * C;
+                        const int t10 = (kc.y1 * Wm + kc.x0) * C, t11 = (kc.y1 * Wm + kc.x1) * C;
+#pragma unroll 4
+                        for (int r = 0; r < kC; ++r) {
+                            const int c = (r + lane) & (kC - 1);
+                            const float v = mine[c];
+                            atomicAdd(&GP[t00 + c], kc.w_nw * v);
+                            atomicAdd(&GP[t01 + c], kc.w_ne * v);
+                            atomicAdd(&GP[t10 + c], kc.w_sw * v);
+                            atomicAdd(&GP[t11 + c], kc.w_se * v);
+                        }
+#pragma unroll
+                        for (int q = 0; q < kC / 4; ++q)
+                            *reinterpret_cast<float4*>(mine + 4 * q) =
+                                make_float4(dx[4 * q] * mat[4 * q], dx[4 * q + 1] * mat[4 * q + 1],
+                                            dx[4 * q + 2] * mat[4 * q + 2], dx[4 * q + 3] * mat[4 * q + 3]);
                         const int lo = s_lo[m];
                         const int i0 = l.x0 - lo, i1 = l.x1 - lo;
-#pragma unroll
-                        for (int c = 0; c < kC; ++c) {
-                            const float gm = dx[c] * vec[m][c], gv = dx[c] * mat[m][c];
-                            atomicAdd(&GP[gswz(kc.y0 * Wm + kc.x0, c)], kc.w_nw * gm);
-                            atomicAdd(&GP[gswz(kc.y0 * Wm + kc.x1, c)], kc.w_ne * gm);
-                            atomicAdd(&GP[gswz(kc.y1 * Wm + kc.x0, c)], kc.w_sw * gm);
-                            atomicAdd(&GP[gswz(kc.y1 * Wm + kc.x1, c)], kc.w_se * gm);
-                            if (i0 >= 0 && i0 < kLineWinTC)
-                                atomicAdd(&gln[(m * kLineWinTC + i0) * C + c], l.w0 * gv);
-                            else
-                                atomicAdd(&p.gfield.line[m][l.x0 * C + c], l.w0 * gv);
-                            if (i1 >= 0 && i1 < kLineWinTC)
-                                atomicAdd(&gln[(m * kLineWinTC + i1) * C + c], l.w1 * gv);
-                            else
-                                atomicAdd(&p.gfield.line[m][l.x1 * C + c], l.w1 * gv);
+                        if (i0 >= 0 && i0 < kLineWinTC && i1 >= 0 && i1 < kLineWinTC) {
+                            float* L0 = gln + (m * kLineWinTC + i0) * C;
+                            float* L1 = gln + (m * kLineWinTC + i1) * C;
+#pragma unroll 4
+                            for (int r = 0; r < kC; ++r) {
+                                const int c = (r + lane) & (kC - 1);
+                                const float v = mine[c];
+                                atomicAdd(L0 + c, l.w0 * v);
+                                atomicAdd(L1 + c, l.w1 * v);
+                            }
+                        } else {  // outside the item's window: straight to global
+                            for (int c = 0; c < kC; ++c) {
+                                atomicAdd(&p.gfield.line[m][l.x0 * C + c], l.w0 * mine[c]);
+                                atomicAdd(&p.gfield.line[m][l.x1 * C + c], l.w1 * mine[c]);
+                            }
                         }
                     }
                 }
@@ -595,15 +680,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
                 const float* src = gpl + p.plane_off[m];
-                for (int i = tid * 4; i < pf; i += kThreadsTC * 4) {
-                    // un-swizzle: quad q of texel tau is stored at quad q ^ (m >> 2),
-                    // element e of it at position e ^ (m & 3), with m = tau & 15
-                    const int tau = i / kC, q = (i % kC) / 4, msk = tau & (kC - 1);
-                    const float4 v = *reinterpret_cast<const float4*>(src + tau * kC + 4 * (q ^ (msk >> 2)));
-                    const float a[4] = {v.x, v.y, v.z, v.w};
-                    const int x = msk & 3;
-                    atomicAdd(reinterpret_cast<float4*>(dst + i), make_float4(a[0 ^ x], a[1 ^ x], a[2 ^ x], a[3 ^ x]));
-                }
+                for (int i = tid * 4; i < pf; i += kThreadsTC * 4)
+                    atomicAdd(reinterpret_cast<float4*>(dst + i), *reinterpret_cast<const float4*>(src + i));
                 const int Ln = p.field.line_len[m];
                 const int lo = s_lo[m];
                 for (int i = tid; i < kLineWinTC * C; i += kThreadsTC) {

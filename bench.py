@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd rays/s"
 WORKLOAD = "C2: 256^3 phantom (200 ellipsoids), 61 tilts x 256^2 detector, octree depth 4 (4096 leaves), " \
-           "rank-16 VM 17^2 planes, decoder 16->64->64->1, 16384-ray batch, 24 samples/leaf-diagonal, FP32"
+           "rank-16 VM 17^2 planes, decoder 16->64->64->1, 16384-ray batch, 24 samples/leaf-diagonal"
 
 
 def parse():
@@ -197,9 +197,6 @@ def run_ours(args, rank, world):
     R = args.rays
     M = cfg.max_samples_per_node
     tree = syn.make_tree(cfg.tree_depth, device="cuda")
-    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
-    params = syn.parameters(geo)
-    opt = torch.optim.Adam(params, lr=1e-3, fused=True)
     nb = 4
     batches = make_batches(cfg, R, nb, 1004 + 1000 * rank)
     # device-resident inputs (value) and pinned host inputs (e2e)
@@ -208,93 +205,107 @@ def run_ours(args, rank, world):
     host_batches = [(torch.from_numpy(o).pin_memory(), torch.from_numpy(d).pin_memory(),
                      torch.from_numpy(y)[None].pin_memory()) for o, d, y in batches]
     stream = torch.cuda.current_stream()
-
-    def step(o, d, y, k):
-        rays = ab.RayList(o, d)
-        img = geo.ProjectRays(tree, rays, M, 1 + k)
-        loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
-        img.backward(gimg)
-        if world > 1:
-            for p in params:
-                dist.all_reduce(p.grad)
-        opt.step()
-        opt.zero_grad(set_to_none=False)
-        return loss
-
-    for k in range(args.warmup):
-        step(*dev_batches[k % nb], k)
-    torch.cuda.synchronize()
-
-    # device-timed region, inputs resident in HBM
-    sampler = ClockSampler(local)
-    sampler.start()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for k in range(args.steps):
-        step(*dev_batches[k % nb], 100 + k)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        dist.barrier()
-
-    # end to end through the public API with host buffers: H2D of the batch,
-    # D2H of the loss, every step
-    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    loss_host = torch.zeros(1, dtype=torch.float64).pin_memory()
-    torch.cuda.synchronize()
-    h0.record(stream)
-    for k in range(args.steps):
-        o, d, y = host_batches[k % nb]
-        og, dg, yg = o.cuda(non_blocking=True), d.cuda(non_blocking=True), y.cuda(non_blocking=True)
-        loss = step(og, dg, yg, 200 + k)
-        loss_host.copy_(loss.reshape(1), non_blocking=True)
-    h1.record(stream)
-    torch.cuda.synchronize()
-    ms_e2e = h0.elapsed_time(h1) / args.steps
-    clocks = sampler.stop()
-    h2d = sum(t.numel() * t.element_size() for t in host_batches[0])
-    d2h = 8
-
-    # roofline of the dominant kernel: forward and backward launches timed alone
     n_slots = int(tree.NumActiveNodes())
     sg = tree.RaySegments(ab.RayList(*dev_batches[0][:2]), M)
-    fwd_b, bwd_b = algorithmic_bytes(cfg, n_slots, R, sg.num_segments)
-    reps = 5
-    f0, f1, b0, b1 = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    o, d, y = dev_batches[0]
-    rays = ab.RayList(o, d)
-    tf = tb = 0.0
-    for k in range(reps):
-        f0.record(stream)
-        img = geo.ProjectRays(tree, rays, M, 7)
-        f1.record(stream)
-        gimg = torch.ones_like(img)
-        b0.record(stream)
-        img.backward(gimg)
-        b1.record(stream)
-        torch.cuda.synchronize()
-        tf += f0.elapsed_time(f1)
-        tb += b0.elapsed_time(b1)
-    tf /= reps
-    tb /= reps
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
+
+    def measure(form, sampler=None):
+        geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
+        bf16 = form == "bf16"
+        if bf16:
+            geo.precision = "bf16"
+            geo.RefreshLowPrecision()
+        params = syn.parameters(geo)
+        opt = torch.optim.Adam(params, lr=1e-3, fused=True)
+
+        def step(o, d, y, k):
+            rays = ab.RayList(o, d)
+            img = geo.ProjectRays(tree, rays, M, 1 + k)
+            loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
+            img.backward(gimg)
+            if world > 1:
+                for p in params:
+                    dist.all_reduce(p.grad)
+            opt.step()
+            opt.zero_grad(set_to_none=False)
+            if bf16:
+                geo.RefreshLowPrecision()
+            return loss
+
+        for k in range(args.warmup):
+            step(*dev_batches[k % nb], k)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(args.steps):
+            step(*dev_batches[k % nb], 100 + k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            dist.barrier()
+        # end to end through the public API with host buffers: H2D of the
+        # batch, D2H of the loss, every step
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        loss_host = torch.zeros(1, dtype=torch.float64).pin_memory()
+        torch.cuda.synchronize()
+        h0.record(stream)
+        for k in range(args.steps):
+            o, d, y = host_batches[k % nb]
+            og, dg, yg = o.cuda(non_blocking=True), d.cuda(non_blocking=True), y.cuda(non_blocking=True)
+            loss = step(og, dg, yg, 200 + k)
+            loss_host.copy_(loss.reshape(1), non_blocking=True)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = h0.elapsed_time(h1) / args.steps
+        clocks = sampler.stop() if sampler else None
+        # forward and backward calls timed alone (CUDA events on the launching stream)
+        reps = 5
+        f0, f1, b0, b1 = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        o, d, y = dev_batches[0]
+        rays = ab.RayList(o, d)
+        tf = tb = 0.0
+        for k in range(reps):
+            f0.record(stream)
+            img = geo.ProjectRays(tree, rays, M, 7)
+            f1.record(stream)
+            gimg = torch.ones_like(img)
+            b0.record(stream)
+            img.backward(gimg)
+            b1.record(stream)
+            torch.cuda.synchronize()
+            tf += f0.elapsed_time(f1)
+            tb += b0.elapsed_time(b1)
+        del geo, opt, params
+        return ms, ms_e2e, tf / reps, tb / reps, clocks
+
+    sampler = ClockSampler(local)
+    ms, ms_e2e, tf, tb, clocks = measure("bf16", sampler)
+    ms32, ms32_e2e, tf32, tb32, _ = measure("fp32")
+
+    esz = 2
+    F = 3 * cfg.channels * cfg.grid * cfg.grid
+    seg_bytes = sg.num_segments * 24 + R * 32
+    fwd_b = n_slots * F * esz + seg_bytes
+    bwd_b = n_slots * F * esz + n_slots * F * 4 + seg_bytes  # BF16 planes read, FP32 gradient written
     dom_ms, dom_bytes, dom_name = (tb, bwd_b, "backward") if tb >= tf else (tf, fwd_b, "forward")
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    h2d = sum(t.numel() * t.element_size() for t in host_batches[0])
 
-    # max over ranks
-    vals = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    vals = torch.tensor([ms, ms_e2e, ms32], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = vals.tolist()
+    ms, ms_e2e, ms32 = vals.tolist()
     if rank != 0:
         return
     launches_per_step = 13
@@ -309,20 +320,26 @@ def run_ours(args, rank, world):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "bf16",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rays_per_gpu_step": R, "samples_per_step": int(sg.num_samples),
-                   "segments_per_step": int(sg.num_segments), "leaves": n_slots,
-                   "parallelism": f"ray data parallel x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (227 MB FP32 factors read and 227 MB of gradients written per step)",
-                   "form": "plain FP32 (CUDA cores), hand-written adjoint, fused leaf-major"},
+        "config": {"workload": WORKLOAD.replace(", FP32", ""), "rays_per_gpu_step": R,
+                   "samples_per_step": int(sg.num_samples), "segments_per_step": int(sg.num_segments),
+                   "leaves": n_slots, "parallelism": f"ray data parallel x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (114 MB BF16 factors read and 227 MB of FP32 gradients written "
+                         "per step, 908 MB of FP32 Adam state)",
+                   "form": "chosen: BF16 factors, tcgen05 decoder GEMMs (FP32 accumulation), hand-written "
+                           "adjoint, fused leaf-major; Adam on FP32 masters"},
         "e2e": {"value": world * R / (ms_e2e * 1e-3), "unit": "rays/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": f"fused {dom_name}", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                     "algorithmic_bytes": dom_bytes, "kernel_ms": dom_ms,
+                "d2h_bytes_per_step": 8},
+        "roofline": {"bound": "hbm", "kernel": f"fused {dom_name} (tcgen05)", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "algorithmic_bytes": dom_bytes,
+                     "kernel_ms": dom_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
         "kernels_ms": {"fused_forward_call": tf, "fused_backward_call": tb},
+        "plain_fp32": {"value": world * R / (ms32 * 1e-3), "unit": "rays/s", "ms_per_step": ms32,
+                       "e2e_value": world * R / (ms32_e2e * 1e-3),
+                       "kernels_ms": {"fused_forward_call": tf32, "fused_backward_call": tb32}},
+        "speedup_vs_plain_fp32": ms32 / ms,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "samples_per_s": world * sg.num_samples / (ms * 1e-3),
