@@ -48,6 +48,7 @@ IntegrateSamplesXRay = ext.IntegrateSamplesXRay
 AccumulateSampleLossPerNode = ext.AccumulateSampleLossPerNode
 MseLossAndGrad = ext.MseLossAndGrad
 DecodeFeatures = ext.DecodeFeatures
+SiddonProject = ext.SiddonProject
 
 __all__ = [
     "ext",
@@ -63,4 +64,5 @@ __all__ = [
     "AccumulateSampleLossPerNode",
     "MseLossAndGrad",
     "DecodeFeatures",
+    "SiddonProject",
 ]

@@ -138,6 +138,8 @@ def _declare(L):
         "atdf_project_node_error": (I32, [ct.POINTER(Tree), P, P, I64, I32, U64, P, I32, P, P, P, SZ, P, P]),
         "atdf_project_forward_noalloc": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, I32,
                                                U64, P, P, P]),
+        "atdf_siddon_project": (I32, [P, I32, I32, I32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), P, P,
+                                      I64, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

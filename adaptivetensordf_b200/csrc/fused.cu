@@ -841,6 +841,8 @@ static int launch_persistent(KernelFn fn, int smem, const FusedParams& p, cudaSt
 {
     if (smem > max_smem_optin()) return ATDF_ERR_UNSUPPORTED;
     ATDF_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ATDF_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
     int dev = 0, sms = 0, per = 0;
     ATDF_CUDA_TRY(cudaGetDevice(&dev));
     ATDF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

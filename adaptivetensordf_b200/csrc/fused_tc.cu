@@ -312,7 +312,7 @@ __device__ __forceinline__ void epilogue_l0(unsigned char* sm, const TCSmem& L, 
     }
 }
 
-__global__ void __launch_bounds__(kThreadsTC) tc_forward_kernel(FusedParams p)
+__global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar_tma;
@@ -752,6 +752,10 @@ static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cu
     const int smem = (int)tcf::TCSmem(p.plane_off[3], bwd).total;
     if (smem > max_optin()) return ATDF_ERR_UNSUPPORTED;
     ATDF_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    // without an explicit carveout the occupancy query assumes a smaller
+    // shared-memory partition and reports one forward CTA per SM
+    ATDF_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
     int dev = 0, sms = 0, per = 0;
     ATDF_CUDA_TRY(cudaGetDevice(&dev));
     ATDF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

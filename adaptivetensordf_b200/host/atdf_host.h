@@ -139,6 +139,12 @@ std::pair<torch::Tensor, torch::Tensor> AccumulateSampleLossPerNode(const Sample
 // Fused MSE loss + gradient of an image against a target.
 std::tuple<torch::Tensor, torch::Tensor> MseLossAndGrad(torch::Tensor image, torch::Tensor target, double scale);
 
+// FP64 Siddon line integrals of a voxel volume [nz, ny, nx] over the box
+// [box_min, box_max] (synthetic tilt series; SceneBase.cpp:904-1000 reads
+// measured ones instead).
+torch::Tensor SiddonProject(torch::Tensor volume, torch::Tensor origin, torch::Tensor direction,
+                            std::vector<double> box_min, std::vector<double> box_max);
+
 int activation_id(const std::string& name);
 void check_status(int status, const char* what);
 void check_dev_error(torch::Tensor err, const char* what);

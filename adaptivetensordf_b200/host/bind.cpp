@@ -132,6 +132,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
     m.def("IntegrateSamplesXRay", &IntegrateSamplesXRay);
     m.def("AccumulateSampleLossPerNode", &AccumulateSampleLossPerNode);
     m.def("MseLossAndGrad", &MseLossAndGrad);
+    m.def("SiddonProject", &SiddonProject, py::arg("volume"), py::arg("origin"), py::arg("direction"),
+          py::arg("box_min") = std::vector<double>{-1, -1, -1}, py::arg("box_max") = std::vector<double>{1, 1, 1});
     m.def(
         "DecodeFeatures",
         [](std::vector<torch::Tensor> weight, std::vector<torch::Tensor> bias, std::string act, std::string last,

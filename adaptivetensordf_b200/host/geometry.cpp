@@ -236,6 +236,24 @@ std::tuple<Tensor, Tensor> MseLossAndGrad(Tensor image, Tensor target, double sc
     return {loss, grad};
 }
 
+Tensor SiddonProject(Tensor volume, Tensor origin, Tensor direction, std::vector<double> box_min,
+                     std::vector<double> box_max)
+{
+    ATDF_CHECK_CUDA(volume);
+    TORCH_CHECK(volume.dim() == 3 && volume.scalar_type() == torch::kFloat32, "volume: [nz, ny, nx] float");
+    TORCH_CHECK(box_min.size() == 3 && box_max.size() == 3, "box_min / box_max: 3 values each");
+    auto v = volume.contiguous();
+    auto o = origin.to(v.device()).to(torch::kFloat32).contiguous();
+    auto d = direction.to(v.device()).to(torch::kFloat32).contiguous();
+    TORCH_CHECK(o.dim() == 2 && o.size(1) == 3 && d.sizes() == o.sizes(), "origin / direction: [R, 3]");
+    auto out = torch::empty({o.size(0)}, v.options().dtype(torch::kFloat64));
+    check_status(atdf_siddon_project(v.data_ptr<float>(), (int32_t)v.size(2), (int32_t)v.size(1),
+                                     (int32_t)v.size(0), box_min.data(), box_max.data(), o.data_ptr<float>(),
+                                     d.data_ptr<float>(), o.size(0), out.data_ptr<double>(), stream_arg()),
+                 "SiddonProject");
+    return out;
+}
+
 // ---------------------------------------------------------------------------
 // Decoder (FCBlock + DecodeFeatures) through a flat parameter vector
 // ---------------------------------------------------------------------------

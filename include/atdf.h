@@ -310,6 +310,17 @@ int atdf_project_forward_noalloc(const atdf_tree_t* tree, const atdf_field_t* fi
                                  int32_t max_samples_per_node, uint64_t jitter_seed, float* image,
                                  int32_t* dev_error, atdf_stream_t stream);
 
+/* ---- synthetic tilt series ------------------------------------------------
+ * FP64 line integrals of a voxel volume [nz][ny][nx] (float) spanning the box
+ * [box_min, box_max] (host double[3] each) along num_rays rays (origin /
+ * direction [R, 3] float): out[r] = sum over traversed voxels of (exit t -
+ * entry t) * value, i.e. exact intersection lengths in units of t. Generates
+ * the projections that the reference reads from measured tilt series
+ * (hyperacorn/csrc/data/SceneBase.cpp:904-1000). */
+int atdf_siddon_project(const float* volume, int32_t nx, int32_t ny, int32_t nz, const double* box_min,
+                        const double* box_max, const float* ray_origin, const float* ray_direction,
+                        int64_t num_rays, double* out, atdf_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
