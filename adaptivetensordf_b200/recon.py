@@ -1,0 +1,332 @@
+"""Tomographic reconstruction driver: trains the tensorial density field on a
+synthetic tilt series with the fused projection and its hand-written
+adjoint, and scores it against the phantom.
+
+It follows the reference trainer's loop for the projection path
+(hyperacorn/src/samples/hyper_train.cpp: TrainStep :920-944 -- rays of a
+shuffled batch, ComputeImage, MSE against the measured pixels, backward,
+optimizer step; the Adam learning rates of Settings.h:161,537 and the per-epoch
+decay of Settings.h:545) and its volume evaluation (Eval_cell_density /
+UniformSampledVolume, hyper_train.cpp:1780-1831, geometry.cpp:478-495:
+the field sampled at voxel centres through the tree's node lookup).
+
+PSNR (stated, since the reference's Saiga PSNR is not available): the
+reconstruction and the phantom are both divided by max(phantom), and
+PSNR = 10 log10(1 / MSE) over all N^3 voxel centres.
+
+Forms:
+  fp32       plain method: FP32 factors, FP32 SIMT fused kernels;
+  bf16       BF16 factor copies, tcgen05 decoder GEMMs with FP32 accumulation;
+  bf16+prop  the bf16 form with the learned proposal sampler
+             (adaptivetensordf_b200.proposal), judged periodically by the
+             uniform sampler; fp32+prop likewise on the FP32 kernels.
+
+    python -m adaptivetensordf_b200.recon --config C1 --form fp32 --epochs 20
+"""
+
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import synthetic as syn
+
+
+# ----------------------------------------------------------------------------
+# data
+# ----------------------------------------------------------------------------
+def voxelize_boxes(ph, N: int, speckle: float = 0.0, seed: int = 1001):
+    """Same volume as synthetic.voxelize (z, y, x order, summed and clamped
+    to 1), evaluated only inside each ellipsoid's bounding box."""
+    c = (np.arange(N) + 0.5) / N * 2 - 1
+    vol = np.zeros((N, N, N), np.float64)
+    for cen, ax, d in zip(ph["centres"], ph["axes"], ph["density"]):
+        lo = np.clip(np.floor((cen - ax + 1) / 2 * N - 0.5).astype(int), 0, N - 1)
+        hi = np.clip(np.ceil((cen + ax + 1) / 2 * N - 0.5).astype(int) + 1, 0, N)
+        if np.any(hi <= lo):
+            continue
+        x = c[lo[0]:hi[0]]
+        y = c[lo[1]:hi[1]]
+        z = c[lo[2]:hi[2]]
+        q = (((z[:, None, None] - cen[2]) / ax[2]) ** 2 + ((y[None, :, None] - cen[1]) / ax[1]) ** 2 +
+             ((x[None, None, :] - cen[0]) / ax[0]) ** 2)
+        vol[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] += d * (q <= 1.0)
+    if speckle > 0:
+        rng = np.random.default_rng(seed + 7)
+        m = rng.random(vol.shape) < speckle
+        vol[m] += rng.uniform(0, 0.2, int(m.sum()))
+    return np.minimum(vol, 1.0)
+
+
+@dataclass
+class TiltSeries:
+    origin: torch.Tensor     # [A * P, 3] float32, device
+    direction: torch.Tensor  # [A * P, 3] float32, device
+    target: torch.Tensor     # [A * P] float32, device (noisy measurement)
+    clean: torch.Tensor      # [A * P] float64, device (noise-free Siddon integrals)
+    volume: torch.Tensor     # [N, N, N] float32 phantom (z, y, x), device
+    angles: np.ndarray
+
+    @property
+    def num_rays(self):
+        return self.origin.shape[0]
+
+
+def make_tilt_series(cfg, device="cuda", noise_seed: int = 1002) -> TiltSeries:
+    """Parallel-beam tilt series of the voxelised phantom: FP64 Siddon line
+    integrals, then (when cfg.noise > 0) a per-tilt multiplicative jitter
+    U[1 - cfg.jitter, 1 + cfg.jitter] and additive N(0, (noise * max y)^2)."""
+    from . import SiddonProject
+
+    ph = syn.ellipsoid_phantom(cfg.ellipsoids, 1001)
+    vol = voxelize_boxes(ph, cfg.volume, cfg.speckle)
+    vol_t = torch.from_numpy(vol.astype(np.float32)).to(device)
+    angles = syn.tilt_angles(cfg)
+    A, P = cfg.angles, cfg.detector * cfg.detector
+    img = np.repeat(np.arange(A), P)
+    pix = np.tile(np.arange(P), A)
+    o, d = syn.parallel_beam_rays(angles, cfg.detector, img, pix)
+    o_t = torch.from_numpy(o).to(device)
+    d_t = torch.from_numpy(d).to(device)
+    clean = SiddonProject(vol_t, o_t, d_t)
+    y = clean.clone()
+    if cfg.noise > 0 or cfg.jitter > 0:
+        rng = np.random.default_rng(noise_seed)
+        mult = rng.uniform(1 - cfg.jitter, 1 + cfg.jitter, A)
+        y = y * torch.from_numpy(mult).to(device).repeat_interleave(P)
+        if cfg.noise > 0:
+            sigma = cfg.noise * float(y.max())
+            y = y + torch.from_numpy(rng.normal(0.0, sigma, A * P)).to(device)
+    return TiltSeries(o_t, d_t, y.float(), clean, vol_t, angles)
+
+
+# ----------------------------------------------------------------------------
+# evaluation
+# ----------------------------------------------------------------------------
+def voxel_centres(N: int, z0: int, z1: int, device="cuda"):
+    c = (torch.arange(N, device=device, dtype=torch.float64) + 0.5) / N * 2 - 1
+    zz, yy, xx = torch.meshgrid(c[z0:z1], c, c, indexing="ij")
+    return torch.stack([xx, yy, zz], -1).reshape(-1, 3).float().contiguous()
+
+
+@torch.no_grad()
+def density_volume(tree, geo, N: int, chunk_points: int = 1 << 21, device="cuda"):
+    """The field's density at the N^3 voxel centres, [N, N, N] (z, y, x)."""
+    out = torch.empty((N, N, N), device=device, dtype=torch.float32)
+    zc = max(1, chunk_points // (N * N))
+    for z0 in range(0, N, zc):
+        z1 = min(N, z0 + zc)
+        pts = voxel_centres(N, z0, z1, device)
+        nid, _ = tree.NodeIdForPositionGPU(pts)
+        dens = geo.SampleVolumeIndirect(tree, pts, nid)
+        out[z0:z1] = dens.reshape(z1 - z0, N, N)
+    return out
+
+
+@torch.no_grad()
+def psnr(tree, geo, phantom: torch.Tensor):
+    N = phantom.shape[0]
+    rec = density_volume(tree, geo, N, device=phantom.device)
+    m = float(phantom.max())
+    mse = float(((rec.double() - phantom.double()) / m).pow(2).mean())
+    return 10.0 * math.log10(1.0 / max(mse, 1e-30))
+
+
+# ----------------------------------------------------------------------------
+# training
+# ----------------------------------------------------------------------------
+@dataclass
+class TrainOptions:
+    epochs: int = 10
+    batch: int = 4096
+    max_samples_per_node: int = 32
+    lr_grid: float = 0.01       # Settings.h:537 lr_exex_grid_adam
+    lr_decoder: float = 5e-4    # Settings.h:161 decoder_lr
+    lr_decay: float = 0.95      # Settings.h:545, per epoch
+    loss_tv: float = 0.0        # plane TV weight (Settings.h:565 loss_tv)
+    init_scale: float = 0.5     # factor init uniform(-s, s) (vm_init_scale)
+    budget: int = 64            # proposal: samples per ray
+    gate: float = 0.01          # proposal: relative L2 projection error allowed vs the uniform judge
+    judge_every: int = 10       # proposal: steps between judge passes while open
+    eval_every: int = 0         # steps between evaluations (0: once per epoch)
+    target_psnr: float = 30.0
+    time_limit: float = 0.0     # seconds of training; 0 = no limit
+    stop_at_target: bool = True
+    order_seed: int = 1004
+
+
+def plane_tv(planes):
+    """TV loss of the plane factors (geometry.h:31-75 TVLoss on the
+    [N, C, H, W] planes, geometry_tensor_qo.cpp:580-582): per spatial axis the
+    mean absolute difference of neighbouring texels, summed over axes and
+    planes."""
+    tv = 0.0
+    for p in planes:
+        tv = tv + (p[:, :, 1:, :] - p[:, :, :-1, :]).abs().mean() + (p[:, :, :, 1:] - p[:, :, :, :-1]).abs().mean()
+    return tv
+
+
+def build_model(cfg, form: str, device="cuda", param_seed: int = 1003, init_scale: float = 0.5):
+    tree = syn.make_tree(cfg.tree_depth, device=device)
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=param_seed, device=device,
+                            init_scale=init_scale)
+    geo.precision = "fp32" if form.startswith("fp32") else "bf16"
+    if geo.precision == "bf16":
+        geo.RefreshLowPrecision()
+    return tree, geo
+
+
+def fit(tree, geo, data: TiltSeries, opt: TrainOptions, device="cuda"):
+    """opt.epochs epochs of uniform-sampling training of an existing model
+    (no evaluation)."""
+    from . import RayList
+
+    adam = torch.optim.Adam([{"params": list(geo.planes) + list(geo.lines), "lr": opt.lr_grid},
+                             {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": opt.lr_decoder}])
+    gen = torch.Generator(device=device).manual_seed(opt.order_seed)
+    n = data.num_rays
+    step = 0
+    for epoch in range(opt.epochs):
+        perm = torch.randperm(n, device=device, generator=gen)
+        for s in range(n // opt.batch):
+            idx = perm[s * opt.batch:(s + 1) * opt.batch]
+            img = geo.ProjectRays(tree, RayList(data.origin[idx], data.direction[idx]), opt.max_samples_per_node,
+                                  (step + 1) * 0x9E3779B1)
+            loss = (img.view(-1) - data.target[idx]).pow(2).mean()
+            adam.zero_grad(set_to_none=True)
+            loss.backward()
+            adam.step()
+            if geo.precision == "bf16":
+                geo.RefreshLowPrecision()
+            step += 1
+    torch.cuda.synchronize()
+
+
+def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device="cuda"):
+    """Train one form; returns (evaluation records, seconds to the target
+    PSNR or None). A record is {t, step, epoch, psnr, loss}, t the training
+    wall time (seconds, GPU-synchronised, evaluations excluded)."""
+    from . import RayList
+
+    tree, geo = build_model(cfg, form, device, init_scale=opt.init_scale)
+    grid_params = list(geo.planes) + list(geo.lines)
+    dec_params = list(geo.decoder_weight) + list(geo.decoder_bias)
+    adam = torch.optim.Adam([{"params": grid_params, "lr": opt.lr_grid},
+                             {"params": dec_params, "lr": opt.lr_decoder}], fused=True)
+    sched = torch.optim.lr_scheduler.ExponentialLR(adam, opt.lr_decay)
+    prop = None
+    if form.endswith("+prop"):
+        from .proposal import ProposalSchedule
+
+        prop = ProposalSchedule(tree, geo, opt.max_samples_per_node, budget=opt.budget, gate=opt.gate,
+                                judge_every=opt.judge_every, device=device)
+
+    n = data.num_rays
+    steps_per_epoch = n // opt.batch
+    gen = torch.Generator(device=device).manual_seed(opt.order_seed)
+    records = []
+    t_train = 0.0
+    step = 0
+    loss_acc = torch.zeros((), device=device, dtype=torch.float64)
+    reached = None
+
+    def evaluate(epoch):
+        nonlocal reached
+        p = psnr(tree, geo, data.volume)
+        rec = {"form": form, "t": t_train, "step": step, "epoch": epoch, "psnr": p,
+               "loss": float(loss_acc) / max(1, step)}
+        if prop is not None:
+            rec.update(prop.stats())
+        records.append(rec)
+        if log:
+            log(rec)
+        if reached is None and p >= opt.target_psnr:
+            reached = t_train
+        return p
+
+    torch.cuda.synchronize()
+    for epoch in range(opt.epochs):
+        perm = torch.randperm(n, device=device, generator=gen)
+        for s in range(steps_per_epoch):
+            t0 = time.perf_counter()
+            idx = perm[s * opt.batch:(s + 1) * opt.batch]
+            rays = RayList(data.origin[idx], data.direction[idx])
+            target = data.target[idx]
+            seed = (step + 1) * 0x9E3779B1
+            if prop is not None:
+                img = prop.project(rays, seed)
+            else:
+                img = geo.ProjectRays(tree, rays, opt.max_samples_per_node, seed)
+            loss = (img.view(-1) - target).pow(2).mean()
+            if opt.loss_tv > 0:
+                loss = loss + opt.loss_tv * plane_tv(geo.planes)
+            adam.zero_grad(set_to_none=True)
+            loss.backward()
+            adam.step()
+            if geo.precision == "bf16":
+                geo.RefreshLowPrecision()
+            loss_acc += loss.detach().double()
+            torch.cuda.synchronize()
+            t_train += time.perf_counter() - t0
+            step += 1
+            if opt.eval_every and step % opt.eval_every == 0:
+                evaluate(epoch)
+                if reached is not None and opt.stop_at_target:
+                    return records, reached
+            if opt.time_limit and t_train >= opt.time_limit:
+                evaluate(epoch)
+                return records, reached
+        sched.step()
+        if not opt.eval_every:
+            evaluate(epoch)
+            if reached is not None and opt.stop_at_target:
+                return records, reached
+    return records, reached
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", default="C1")
+    ap.add_argument("--form", default="fp32", choices=["fp32", "bf16", "bf16+prop", "fp32+prop"])
+    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--samples", type=int, default=0, help="max samples per node (0: config value)")
+    ap.add_argument("--eval-every", type=int, default=0)
+    ap.add_argument("--target", type=float, default=30.0)
+    ap.add_argument("--time-limit", type=float, default=0.0)
+    ap.add_argument("--lr-grid", type=float, default=0.01)
+    ap.add_argument("--lr-decoder", type=float, default=5e-4)
+    ap.add_argument("--no-stop", action="store_true")
+    ap.add_argument("--tv", type=float, default=0.0)
+    ap.add_argument("--init-scale", type=float, default=0.5)
+    ap.add_argument("--noise", type=float, default=-1.0, help="override the config's noise level")
+    ap.add_argument("--budget", type=int, default=64)
+    ap.add_argument("--gate", type=float, default=0.01)
+    ap.add_argument("--judge-every", type=int, default=10)
+    a = ap.parse_args()
+    cfg = syn.CONFIGS[a.config]
+    if a.noise >= 0:
+        cfg = dataclasses.replace(cfg, noise=a.noise, jitter=0.0 if a.noise == 0 else cfg.jitter)
+    t0 = time.perf_counter()
+    data = make_tilt_series(cfg)
+    torch.cuda.synchronize()
+    print(json.dumps({"data_s": time.perf_counter() - t0, "rays": data.num_rays}), flush=True)
+    opt = TrainOptions(epochs=a.epochs, batch=a.batch or cfg.rays_per_batch,
+                       max_samples_per_node=a.samples or cfg.max_samples_per_node, eval_every=a.eval_every,
+                       target_psnr=a.target, time_limit=a.time_limit, stop_at_target=not a.no_stop,
+                       lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, loss_tv=a.tv, init_scale=a.init_scale,
+                       budget=a.budget, gate=a.gate, judge_every=a.judge_every)
+    recs, reached = train(cfg, a.form, data, opt, log=lambda r: print(json.dumps(r), flush=True))
+    print(json.dumps({"form": a.form, "config": a.config, "seconds_to_target": reached, "target": a.target,
+                      "final_psnr": recs[-1]["psnr"] if recs else None}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
