@@ -140,6 +140,21 @@ def _declare(L):
                                                U64, P, P, P]),
         "atdf_siddon_project": (I32, [P, I32, I32, I32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), P, P,
                                       I64, P, P]),
+        "atdf_project_forward_binned": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, I32,
+                                              U64, P, P, P, SZ, P, P]),
+        "atdf_project_segments": (I32, [ct.POINTER(Tree), P, P, I64, I32, I64, P, SZ, ct.POINTER(Segments), P, P]),
+        "atdf_project_segment_view": (I32, [I64, I32, I64, P, SZ, ct.POINTER(Segments)]),
+        "atdf_project_forward_samples": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, P, P,
+                                               P, P, SZ, P, P]),
+        "atdf_project_backward_samples": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, P,
+                                                P, P, ct.POINTER(FieldGrad), ct.POINTER(MlpGrad), P, SZ, P, P]),
+        "atdf_proposal_features": (I32, [ct.POINTER(Tree), ct.POINTER(Segments), P, P, P, P, P, P]),
+        "atdf_proposal_mlp_forward": (I32, [ct.POINTER(Mlp), ct.POINTER(Segments), P, P, P]),
+        "atdf_proposal_mlp_backward": (I32, [ct.POINTER(Mlp), ct.POINTER(Segments), P, P, ct.POINTER(MlpGrad), P]),
+        "atdf_proposal_allocate": (I32, [ct.POINTER(Segments), I64, P, I32, F32, P]),
+        "atdf_proposal_samples": (I32, [ct.POINTER(Segments), P, F32, U64, P, P, I64, P, P]),
+        "atdf_proposal_loss": (I32, [ct.POINTER(Segments), P, P, P, F32, P, P, P, P, I64, P, P]),
+        "atdf_proposal_occupancy": (I32, [P, P, I64, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

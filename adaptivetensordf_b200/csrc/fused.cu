@@ -391,11 +391,12 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
             float f[NF];
 #pragma unroll
             for (int i = 0; i < NF; ++i) f[i] = 0.0f;
-            float w = 0.0f;
+            float w = 0.0f, ts = 0.0f;
             int si = -1;
             if (valid) {
                 const SampleState st = sample_state(p, tab, it, k);
                 w = st.w;
+                ts = st.t;
                 si = st.si;
                 if (real) {
                     const SampleGeo g = sample_geo_fast(p, tab, st.si, st.pos);
@@ -433,6 +434,7 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
             if (q == 0 && valid) {
                 const float rho = act_fwd(lact, z, beta);
                 atomicAdd(&tab.acc[si], __fmul_rn(rho, w));
+                if (p.bins) add_to_bins(p, tab, si, ts, __fmul_rn(rho, w));
             }
             __syncthreads();
         }
@@ -470,7 +472,8 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
     constexpr int PARTS = kThreads / H;  // bias / last-layer partial sums
     constexpr int SPP = kT / PARTS;
     const int bn = tid % H, bpart = tid / H;
-    float gb0 = 0.0f, gb1 = 0.0f, gwl = 0.0f, gbl = 0.0f;
+    float gb0 = 0.0f, gb1 = 0.0f, gwl = 0.0f;
+    double gbl = 0.0;  // one scalar summed over every sample: FP64 against cancellation
 
     while (true) {
         const ItemInfo it = next_item(p, 1, sm, tab, &bar, s_ctl, true);
@@ -574,7 +577,7 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
                 const int ss = bpart * SPP + i;
                 gwl = fmaf(sm[L.sz + ss], hlast_s[ss * H + bn], gwl);
             }
-            if (tid < kT) gbl += sm[L.sz + tid];
+            if (tid < kT) gbl += (double)sm[L.sz + tid];
             __syncthreads();
             // dA of the last hidden layer: dz * Wl * act'(pre); k-major (in
             // place of the pre-activation) and sample-major copies
@@ -710,7 +713,11 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
     }
     atomicAdd(&p.gmlp.bias[0][bn], gb0);
     atomicAdd(&p.gmlp.weight[NH][bn], gwl);
-    if (tid < kT) atomicAdd(&p.gmlp.bias[NH][0], gbl);
+    static_assert(kT == 32, "the last-layer bias partials live in warp 0");
+    if (tid < 32) {
+        for (int off = 16; off > 0; off >>= 1) gbl += __shfl_down_sync(0xffffffffu, gbl, off);
+        if (tid == 0) atomicAdd(&p.gmlp.bias[NH][0], (float)gbl);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -834,6 +841,9 @@ static int prepare(const atdf_tree_t* tree, const atdf_field_t* field, const atd
     p.dir = dir;
     p.R = R;
     p.grad_image = nullptr;
+    p.xt = nullptr;
+    p.xw = nullptr;
+    p.bins = nullptr;
     return ATDF_OK;
 }
 
@@ -853,25 +863,15 @@ static int launch_persistent(KernelFn fn, int smem, const FusedParams& p, cudaSt
     return ATDF_OK;
 }
 
-}  // namespace atdf
 
-using namespace atdf;
-
-extern "C" {
-
-int atdf_project_workspace_size(int64_t num_rays, int32_t max_depth, int32_t ns, int64_t num_slots,
-                                int32_t out_channels, size_t* bytes)
-{
-    if (!bytes || num_rays < 0 || max_depth < 0 || num_slots < 0 || (ns != 4 && ns != 8) || out_channels != 1)
-        return ATDF_ERR_INVALID_ARGUMENT;
-    *bytes = ws_layout(num_rays, max_depth, num_slots, nullptr, nullptr);
-    return ATDF_OK;
-}
-
-int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
-                         const float* ray_origin, const float* ray_direction, int64_t num_rays,
-                         int32_t max_samples_per_node, uint64_t jitter_seed, float* image, void* workspace,
-                         size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+// Forward projection. compute_segments: derive the ray/leaf segments (and the
+// uniform per-node sample counts) into the workspace; otherwise use the
+// segments already there (atdf_project_segments) with caller-placed samples.
+static int project_forward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                           const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                           int32_t max_samples_per_node, uint64_t jitter_seed, bool compute_segments,
+                           const float* xt, const float* xw, float* bins, float* image, void* workspace,
+                           size_t workspace_bytes, int32_t* dev_error, cudaStream_t s)
 {
     FusedParams p;
     const Variant* var = nullptr;
@@ -881,11 +881,16 @@ int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, con
     if (num_rays >= ((int64_t)1 << 31)) return ATDF_ERR_UNSUPPORTED;
     p.seed = jitter_seed;
     p.err = dev_error;
-    cudaStream_t s = (cudaStream_t)stream;
+    p.xt = xt;
+    p.xw = xw;
+    p.bins = bins;
     const Ws& w = p.ws;
-    st = launch_ray_segments(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, ws_segments(w),
-                             dev_error, s);
-    if (st != ATDF_OK) return st;
+    if (compute_segments) {
+        st = launch_ray_segments(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, ws_segments(w),
+                                 dev_error, s);
+        if (st != ATDF_OK) return st;
+    }
+    if (bins) ATDF_CUDA_TRY(cudaMemsetAsync(bins, 0, (size_t)w.cap * kBins * sizeof(float), s));
     ATDF_CUDA_TRY(cudaMemsetAsync(w.slot_offset, 0, (w.nslot + 2) * 4, s));
     ATDF_CUDA_TRY(cudaMemsetAsync(w.slot_cursor, 0, (w.nslot + 1) * 4, s));
     ATDF_CUDA_TRY(cudaMemsetAsync(w.counters, 0, 8 * 4, s));
@@ -908,13 +913,13 @@ int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, con
     return ATDF_OK;
 }
 
-int atdf_project_backward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
-                          const float* ray_origin, const float* ray_direction, int64_t num_rays,
-                          int32_t max_samples_per_node, uint64_t jitter_seed, const float* grad_image,
-                          const atdf_field_grad_t* grad_field, const atdf_mlp_grad_t* grad_mlp, void* workspace,
-                          size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+// Backward (recomputes every sample; reuses the forward's workspace).
+static int project_backward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                            const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                            uint64_t jitter_seed, const float* xt, const float* xw, const float* grad_image,
+                            const atdf_field_grad_t* grad_field, const atdf_mlp_grad_t* grad_mlp, void* workspace,
+                            size_t workspace_bytes, int32_t* dev_error, cudaStream_t s)
 {
-    (void)max_samples_per_node;
     FusedParams p;
     const Variant* var = nullptr;
     int st = prepare(tree, field, mlp, ray_origin, ray_direction, num_rays, workspace, workspace_bytes, p, var);
@@ -930,7 +935,8 @@ int atdf_project_backward(const atdf_tree_t* tree, const atdf_field_t* field, co
     p.grad_image = grad_image;
     p.gfield = *grad_field;
     p.gmlp = *grad_mlp;
-    cudaStream_t s = (cudaStream_t)stream;
+    p.xt = xt;
+    p.xw = xw;
     for (int m = 0; m < 3; ++m) {
         const size_t pf = (size_t)field->plane_h[m] * field->plane_w[m] * field->channels * field->num_slots;
         ATDF_CUDA_TRY(cudaMemsetAsync(grad_field->plane[m], 0, pf * 4, s));
@@ -943,6 +949,104 @@ int atdf_project_backward(const atdf_tree_t* tree, const atdf_field_t* field, co
     }
     ATDF_CUDA_TRY(cudaMemsetAsync(p.ws.counters + 1, 0, 4, s));
     return var ? launch_persistent(var->bwd, var->smem(p.plane_off[3], true), p, s) : launch_tc_backward(p, s);
+}
+
+}  // namespace atdf
+
+using namespace atdf;
+
+extern "C" {
+
+int atdf_project_workspace_size(int64_t num_rays, int32_t max_depth, int32_t ns, int64_t num_slots,
+                                int32_t out_channels, size_t* bytes)
+{
+    if (!bytes || num_rays < 0 || max_depth < 0 || num_slots < 0 || (ns != 4 && ns != 8) || out_channels != 1)
+        return ATDF_ERR_INVALID_ARGUMENT;
+    *bytes = ws_layout(num_rays, max_depth, num_slots, nullptr, nullptr);
+    return ATDF_OK;
+}
+
+int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                         const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                         int32_t max_samples_per_node, uint64_t jitter_seed, float* image, void* workspace,
+                         size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+{
+    return project_forward(tree, field, mlp, ray_origin, ray_direction, num_rays, max_samples_per_node, jitter_seed,
+                           true, nullptr, nullptr, nullptr, image, workspace, workspace_bytes, dev_error,
+                           (cudaStream_t)stream);
+}
+
+int atdf_project_forward_binned(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                int32_t max_samples_per_node, uint64_t jitter_seed, float* image, float* seg_bins,
+                                void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+{
+    if (!seg_bins) return ATDF_ERR_INVALID_ARGUMENT;
+    return project_forward(tree, field, mlp, ray_origin, ray_direction, num_rays, max_samples_per_node, jitter_seed,
+                           true, nullptr, nullptr, seg_bins, image, workspace, workspace_bytes, dev_error,
+                           (cudaStream_t)stream);
+}
+
+int atdf_project_segments(const atdf_tree_t* tree, const float* ray_origin, const float* ray_direction,
+                          int64_t num_rays, int32_t max_samples_per_node, int64_t num_slots, void* workspace,
+                          size_t workspace_bytes, atdf_segments_t* view, int32_t* dev_error, atdf_stream_t stream)
+{
+    if (!tree || !workspace || !view || num_rays < 0 || num_slots < 0 ||
+        (num_rays > 0 && (!ray_origin || !ray_direction)))
+        return ATDF_ERR_INVALID_ARGUMENT;
+    if (num_rays >= ((int64_t)1 << 31)) return ATDF_ERR_UNSUPPORTED;
+    const size_t need = ws_layout(num_rays, tree->max_depth, num_slots, nullptr, nullptr);
+    if (workspace_bytes < need) return ATDF_ERR_WORKSPACE;
+    Ws w;
+    ws_layout(num_rays, tree->max_depth, num_slots, (char*)workspace, &w);
+    *view = ws_segments(w);
+    return launch_ray_segments(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, *view, dev_error,
+                               (cudaStream_t)stream);
+}
+
+int atdf_project_segment_view(int64_t num_rays, int32_t max_depth, int64_t num_slots, void* workspace,
+                              size_t workspace_bytes, atdf_segments_t* view)
+{
+    if (!workspace || !view || num_rays < 0 || max_depth < 0 || num_slots < 0) return ATDF_ERR_INVALID_ARGUMENT;
+    const size_t need = ws_layout(num_rays, max_depth, num_slots, nullptr, nullptr);
+    if (workspace_bytes < need) return ATDF_ERR_WORKSPACE;
+    Ws w;
+    ws_layout(num_rays, max_depth, num_slots, (char*)workspace, &w);
+    *view = ws_segments(w);
+    return ATDF_OK;
+}
+
+int atdf_project_forward_samples(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                 const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                 const float* sample_t, const float* sample_w, float* image, void* workspace,
+                                 size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+{
+    if (num_rays > 0 && (!sample_t || !sample_w)) return ATDF_ERR_INVALID_ARGUMENT;
+    return project_forward(tree, field, mlp, ray_origin, ray_direction, num_rays, 0, 0, false, sample_t, sample_w,
+                           nullptr, image, workspace, workspace_bytes, dev_error, (cudaStream_t)stream);
+}
+
+int atdf_project_backward(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                          const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                          int32_t max_samples_per_node, uint64_t jitter_seed, const float* grad_image,
+                          const atdf_field_grad_t* grad_field, const atdf_mlp_grad_t* grad_mlp, void* workspace,
+                          size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+{
+    (void)max_samples_per_node;
+    return project_backward(tree, field, mlp, ray_origin, ray_direction, num_rays, jitter_seed, nullptr, nullptr,
+                            grad_image, grad_field, grad_mlp, workspace, workspace_bytes, dev_error,
+                            (cudaStream_t)stream);
+}
+
+int atdf_project_backward_samples(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                  const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                  const float* sample_t, const float* sample_w, const float* grad_image,
+                                  const atdf_field_grad_t* grad_field, const atdf_mlp_grad_t* grad_mlp,
+                                  void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream)
+{
+    if (num_rays > 0 && (!sample_t || !sample_w)) return ATDF_ERR_INVALID_ARGUMENT;
+    return project_backward(tree, field, mlp, ray_origin, ray_direction, num_rays, 0, sample_t, sample_w, grad_image,
+                            grad_field, grad_mlp, workspace, workspace_bytes, dev_error, (cudaStream_t)stream);
 }
 
 int atdf_project_node_error(const atdf_tree_t* tree, const float* ray_origin, const float* ray_direction,

@@ -12,7 +12,7 @@ namespace atdf {
 
 constexpr int kSegItem = 64;          // segments per work item
 constexpr int kLineWin = 64;          // line-gradient window entries per line
-constexpr int kSegTabArrays = 18;     // arrays of the per-item segment table
+constexpr int kSegTabArrays = 19;     // arrays of the per-item segment table
 constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4);  // floats of the per-item table
 
 // ---------------------------------------------------------------------------
@@ -163,7 +163,17 @@ struct FusedParams {
     int32_t* err;
     int plane_off[4];  // float offsets of the three planes in shared memory (+ total)
     float roi_inv;     // 1 / (roi_max.x - roi_min.x) when a power of two, else 0
+    // Caller-placed samples (null: the uniform per-node rule): t and weight
+    // of every sample in canonical order, indexed by the ray's sample offset
+    // plus the segment's first sample plus j.
+    const float* xt;
+    const float* xw;
+    // Forward only (nullable): rho * w of each sample added into kBins equal
+    // bins of its segment, [segment][kBins].
+    float* bins;
 };
+
+constexpr int kBins = ATDF_PROPOSAL_BINS;
 
 // Per-item segment table in shared memory.
 struct SegTab {
@@ -179,6 +189,7 @@ struct SegTab {
     float* bmin[3];
     float* size[3];
     float* inv[3];  // 1 / size when size is a power of two, else 0
+    int* first;     // global index of the segment's first sample (caller-placed samples)
 };
 
 __device__ __forceinline__ SegTab seg_tab(float* base)
@@ -200,6 +211,7 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
         t.size[k] = base + (12 + k) * S;
         t.inv[k] = base + (15 + k) * S;
     }
+    t.first = ib + 18 * S;
     return t;
 }
 
@@ -279,6 +291,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
         tab.tmax[tid] = tmax;
         tab.step[tid] = __fdiv_rn(__fsub_rn(tmax, tmin), (float)n);  // sample_t's step
         tab.acc[tid] = want_dI ? p.grad_image[w.ray[sid]] : 0.0f;
+        tab.first[tid] = p.xt ? (int)(w.ray_sample_offset[w.ray[sid]] + w.first[sid]) : 0;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
@@ -315,6 +328,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
 struct SampleState {
     int si;
     float w;
+    float t;
     float pos[3];
     int node;
 };
@@ -352,11 +366,20 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
     const int r = tab.ray[s.si];
     s.node = tab.node[s.si];
     const float tmin = tab.tmin[s.si], tmax = tab.tmax[s.si], step = tab.step[s.si];
-    const float t = sample_t_step(tmin, step, j, sample_a(nullptr, 0, p.seed, r, s.node, j));
-    const float tp = j > 0 ? sample_t_step(tmin, step, j - 1, sample_a(nullptr, 0, p.seed, r, s.node, j - 1)) : 0.0f;
-    const float tn =
-        j < n - 1 ? sample_t_step(tmin, step, j + 1, sample_a(nullptr, 0, p.seed, r, s.node, j + 1)) : 0.0f;
-    s.w = sample_w(tmin, tmax, n, j, tp, t, tn);
+    float t;
+    if (p.xt) {
+        const int gi = tab.first[s.si] + j;
+        t = p.xt[gi];
+        s.w = p.xw[gi];
+    } else {
+        t = sample_t_step(tmin, step, j, sample_a(nullptr, 0, p.seed, r, s.node, j));
+        const float tp =
+            j > 0 ? sample_t_step(tmin, step, j - 1, sample_a(nullptr, 0, p.seed, r, s.node, j - 1)) : 0.0f;
+        const float tn =
+            j < n - 1 ? sample_t_step(tmin, step, j + 1, sample_a(nullptr, 0, p.seed, r, s.node, j + 1)) : 0.0f;
+        s.w = sample_w(tmin, tmax, n, j, tp, t, tn);
+    }
+    s.t = t;
 #pragma unroll
     for (int k2 = 0; k2 < 3; ++k2) s.pos[k2] = __fadd_rn(p.origin[3 * r + k2], __fmul_rn(p.dir[3 * r + k2], t));
     return s;
@@ -385,6 +408,15 @@ __device__ __forceinline__ SampleGeo sample_geo_fast(const FusedParams& p, const
     g.lu[1] = loc[1];
     g.lu[2] = pos[2];
     return g;
+}
+
+// Adds rho * w of a sample at t into its segment's bins (forward, optional).
+__device__ __forceinline__ void add_to_bins(const FusedParams& p, const SegTab& tab, int si, float t, float v)
+{
+    const float tmin = tab.tmin[si], len = tab.tmax[si] - tmin;
+    int b = len > 0.0f ? (int)((t - tmin) / len * (float)kBins) : 0;
+    b = b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+    atomicAdd(&p.bins[(int64_t)tab.id[si] * kBins + b], v);
 }
 
 __device__ __forceinline__ void item_box(const FusedParams& p, int node, float* bmin, float* bmax)

@@ -272,17 +272,19 @@ __device__ __forceinline__ uint32_t trow(uint32_t base, int col)
 // Forward sample features of tile row t into HB (X columns); returns validity.
 __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned char* sm, const TCSmem& L,
                                               const SegTab& tab, const ItemInfo& it, bool real, int h, int k,
-                                              int t, float& w, int& si, SampleGeo& g)
+                                              int t, float& w, int& si, SampleGeo& g, float& ts)
 {
     const bool valid = k < it.total;
     float f[kC];
 #pragma unroll
     for (int i = 0; i < kC; ++i) f[i] = 0.0f;
     w = 0.0f;
+    ts = 0.0f;
     si = -1;
     if (valid) {
         const SampleState st = sample_state(p, tab, it, k);
         w = st.w;
+        ts = st.t;
         si = st.si;
         if (real) {
             g = sample_geo_fast(p, tab, st.si, st.pos);
@@ -354,10 +356,10 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
         }
         alive = __syncthreads_and(alive);
         for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
-            float w;
+            float w, ts;
             int si;
             SampleGeo g;
-            const bool valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g);
+            const bool valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g, ts);
             tc::fence_smem_to_async();
             tc::fence_before_sync();
             half_barrier(h);
@@ -388,7 +390,11 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
 #pragma unroll
                 for (int i = 0; i < 16; ++i) z = fmaf(silu(v[i] + bb[i]), ww[i], z);
             }
-            if (valid) atomicAdd(&tab.acc[si], act_fwd(lact, z, beta) * w);
+            if (valid) {
+                const float v = act_fwd(lact, z, beta) * w;
+                atomicAdd(&tab.acc[si], v);
+                if (p.bins) add_to_bins(p, tab, si, ts, v);
+            }
             tc::fence_before_sync();
             half_barrier(h);
         }
@@ -476,9 +482,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
         for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
             bool valid = false;
             SampleGeo g;
-            float w;
+            float w, ts;
             int si;
-            valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g);
+            valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g, ts);
             const float dIw = valid ? tab.acc[si] * w : 0.0f;
             tc::fence_smem_to_async();
             tc::fence_before_sync();

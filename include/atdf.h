@@ -291,6 +291,109 @@ int atdf_project_node_error(const atdf_tree_t* tree, const float* ray_origin, co
                             const float* per_ray_loss, int32_t out_channels, double* loss_sum, double* weight_sum,
                             void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
 
+/* ---- learned proposal sampler --------------------------------------------
+ * No counterpart in the reference, which always places max_samples_per_node
+ * uniform samples in every crossed leaf (HyperTree.cu:266-514). A proposal
+ * MLP (ATDF_PROPOSAL_INPUTS -> 64 x (1..3) SiLU -> ATDF_PROPOSAL_OUTPUTS)
+ * maps each ray/leaf segment to 32 bin logits of a piecewise-constant sample
+ * density over the segment plus one mass logit (predicted integral =
+ * softplus(logit) * segment length). Leaf occupancy is kept per node as
+ * ATDF_PROPOSAL_OCC floats: the mean density of its 8 octants (index = x>0
+ * | (y>0)<<1 | (z>0)<<2 in leaf-local coordinates) and of the whole leaf. */
+#define ATDF_PROPOSAL_BINS 32
+#define ATDF_PROPOSAL_OUTPUTS 33
+#define ATDF_PROPOSAL_INPUTS 16
+#define ATDF_PROPOSAL_OCC 9
+
+/* atdf_project_forward that also adds each sample's rho * w into 32 equal
+ * bins of its segment: seg_bins [segment capacity][32] (zero-filled by the
+ * call; capacity and order as in the workspace's segment view). */
+int atdf_project_forward_binned(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                int32_t max_samples_per_node, uint64_t jitter_seed, float* image, float* seg_bins,
+                                void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
+
+/* Ray/leaf segments (with the uniform per-node sample counts) into a fused
+ * workspace sized by atdf_project_workspace_size; *view receives the
+ * workspace's segment arrays. A caller may then overwrite nsamp, first,
+ * ray_sample_offset and totals[1..2] (atdf_proposal_allocate does) and
+ * project with caller-placed samples. */
+int atdf_project_segments(const atdf_tree_t* tree, const float* ray_origin, const float* ray_direction,
+                          int64_t num_rays, int32_t max_samples_per_node, int64_t num_slots, void* workspace,
+                          size_t workspace_bytes, atdf_segments_t* view, int32_t* dev_error, atdf_stream_t stream);
+
+/* The segment arrays inside a fused workspace (no device work). */
+int atdf_project_segment_view(int64_t num_rays, int32_t max_depth, int64_t num_slots, void* workspace,
+                              size_t workspace_bytes, atdf_segments_t* view);
+
+/* Forward projection over the workspace's segments with caller-placed
+ * samples: sample_t / sample_w [total samples] in canonical order (index =
+ * ray_sample_offset[ray] + first[segment] + j). */
+int atdf_project_forward_samples(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                 const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                 const float* sample_t, const float* sample_w, float* image, void* workspace,
+                                 size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
+
+/* Adjoint of atdf_project_forward_samples (same workspace and samples). */
+int atdf_project_backward_samples(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                  const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                  const float* sample_t, const float* sample_w, const float* grad_image,
+                                  const atdf_field_grad_t* grad_field, const atdf_mlp_grad_t* grad_mlp,
+                                  void* workspace, size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
+
+/* Proposal inputs per segment, features [segment capacity][16]: leaf-local
+ * entry point (3), leaf-local exit point (3), segment length / leaf
+ * diagonal, the leaf's mean occupancy, its 8 octant occupancies
+ * (occupancy [num_nodes][9], nullable: zeros). Rows from totals[0] on are
+ * untouched. */
+int atdf_proposal_features(const atdf_tree_t* tree, const atdf_segments_t* segments, const float* ray_origin,
+                           const float* ray_direction, const float* occupancy, float* features, int32_t* dev_error,
+                           atdf_stream_t stream);
+
+/* The proposal MLP over the totals[0] segment rows (count read on the
+ * device): logits [capacity][33] = MLP(features). mlp: 16 -> 64 x (1..3) ->
+ * 33, SiLU hidden, identity last (else ATDF_ERR_UNSUPPORTED). */
+int atdf_proposal_mlp_forward(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
+                              float* logits, atdf_stream_t stream);
+
+/* Its adjoint: OVERWRITES grad_mlp with the weight and bias gradients for
+ * grad_logits [capacity][33] (rows < totals[0]). */
+int atdf_proposal_mlp_backward(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
+                               const float* grad_logits, const atdf_mlp_grad_t* grad_mlp, atdf_stream_t stream);
+
+/* Splits a budget of samples per ray over its segments: n = 1 +
+ * floor((budget - segments of the ray) * share), share = (1 - mass_mix) *
+ * predicted mass share + mass_mix * length share. Overwrites nsamp, first,
+ * ray_sample_offset, totals[1] (samples) and totals[2] (max per ray). A ray
+ * gets max(budget, its segment count) samples at most. */
+int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, const float* logits, int32_t budget,
+                           float mass_mix, atdf_stream_t stream);
+
+/* Sample t and weight of every segment's nsamp samples: stratified
+ * inverse-CDF draws u_j = (j + a_j) / n (a_j the interval jitter hash of
+ * seed, 0.5 for seed 0) from q = (1 - bin_mix) softmax(bin logits) + bin_mix
+ * / 32 over 32 equal bins; weight = 1 / (n q(t)) in units of t. Unbiased for
+ * any proposal because q > 0 everywhere (bin_mix in (0, 1]). */
+int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, uint64_t seed,
+                          float* sample_t, float* sample_w, int64_t sample_capacity, int32_t* dev_error,
+                          atdf_stream_t stream);
+
+/* Training loss of the proposal against seg_bins of a uniform binned forward
+ * on the same segments: mean over segments of the cross-entropy of the
+ * normalised bins vs softmax(bin logits) plus mass_weight * (log(m_hat +
+ * 1e-4) - log(m + 1e-4))^2. Writes grad_logits (rows < totals[0]),
+ * OVERWRITES *loss (device double) and node_mass / node_len [num_nodes][9]
+ * with the target mass and crossed length per leaf octant and leaf (FP64;
+ * bin centres placed by the features' entry / exit points). */
+int atdf_proposal_loss(const atdf_segments_t* segments, const float* features, const float* seg_bins,
+                       const float* logits, float mass_weight, float* grad_logits, double* loss, double* node_mass,
+                       double* node_len, int64_t num_nodes, int32_t* dev_error, atdf_stream_t stream);
+
+/* occupancy[i] = node_mass[i] / node_len[i] where node_len[i] > 0, over
+ * num_nodes * 9 entries; other entries are kept. */
+int atdf_proposal_occupancy(const double* node_mass, const double* node_len, int64_t num_nodes, float* occupancy,
+                            atdf_stream_t stream);
+
 /* ---- forward projection without device allocation ----------------------
  * No counterpart in the reference (it allocates with torch on every call).
  * For callers that cannot call cudaMalloc (a plugin whose host framework owns
