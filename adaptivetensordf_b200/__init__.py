@@ -49,6 +49,7 @@ AccumulateSampleLossPerNode = ext.AccumulateSampleLossPerNode
 MseLossAndGrad = ext.MseLossAndGrad
 DecodeFeatures = ext.DecodeFeatures
 SiddonProject = ext.SiddonProject
+ProposalSampler = ext.ProposalSampler
 
 __all__ = [
     "ext",
@@ -65,4 +66,5 @@ __all__ = [
     "MseLossAndGrad",
     "DecodeFeatures",
     "SiddonProject",
+    "ProposalSampler",
 ]

@@ -132,6 +132,46 @@ struct GeometryTensorQO {
                                                                              torch::Tensor target);
 };
 
+// Learned proposal sampler (no counterpart in the reference, which places
+// max_samples_per_node uniform samples in every crossed leaf,
+// HyperTree.cu:266-514). A small MLP maps each ray/leaf segment (leaf-local
+// entry and exit points, the relative length, the leaf's occupancy as a whole
+// and per octant) to a 32-bin sample density over the segment and the
+// segment's mass; each ray's budget of samples is split by predicted mass and
+// drawn by stratified inverse-CDF sampling with weights 1 / (n q), so
+// projections stay unbiased. The network trains online on the bins of rho * w
+// of uniform passes (ProjectUniformBinned), which also judge it. No call
+// reads device memory back to the host unless check_errors is set.
+class ProposalSampler {
+   public:
+    ProposalSampler(int64_t num_nodes, int64_t hidden, int64_t hidden_layers, int64_t seed, const std::string& device);
+
+    // Projection through proposal-placed samples (autograd over field + decoder).
+    torch::Tensor Project(HyperTreeBase& tree, GeometryTensorQO& geo, const RayList& rays, uint64_t jitter_seed);
+    // Uniform projection (ProjectRays) that also keeps the per-segment bins
+    // of rho * w as the proposal's next training target.
+    torch::Tensor ProjectUniformBinned(HyperTreeBase& tree, GeometryTensorQO& geo, const RayList& rays,
+                                       int max_samples_per_node, uint64_t jitter_seed);
+    // Proposal loss on the last binned pass; sets weight[l].grad() and
+    // bias[l].grad() and refreshes the leaf occupancy. Returns the loss
+    // (device FP64 scalar).
+    torch::Tensor ComputeGradients(HyperTreeBase& tree);
+    std::vector<torch::Tensor> parameters() const;
+
+    std::vector<torch::Tensor> weight, bias;  // [out, in] / [out], FP32
+    torch::Tensor occupancy;                  // [num_nodes, 9] float: 8 octants + whole leaf
+    int64_t budget = 64;
+    double mass_mix = 0.25, bin_mix = 0.2, mass_weight = 0.1;
+    bool check_errors = false;  // read the device error words after each call (synchronises)
+
+   private:
+    torch::Tensor logits_for(HyperTreeBase& tree, const atdf_segments_t& view, const RayList& rays,
+                             torch::Tensor* features_out);
+    torch::Tensor last_ws_, last_bins_, flat_, err_;
+    RayList last_rays_;
+    int64_t last_slots_ = 0;
+};
+
 // AccumulateSampleLossPerNode (geometry.h:326-327) in FP64.
 std::pair<torch::Tensor, torch::Tensor> AccumulateSampleLossPerNode(const SampleList& samples,
                                                                     torch::Tensor per_ray_loss, int64_t num_nodes);

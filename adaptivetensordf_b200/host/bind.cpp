@@ -126,6 +126,25 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def("ProjectNodeError", &GeometryTensorQO::ProjectNodeError, py::arg("tree"), py::arg("rays"),
              py::arg("max_samples_per_node"), py::arg("jitter_seed"), py::arg("target"));
 
+    py::class_<ProposalSampler>(m, "ProposalSampler")
+        .def(py::init<int64_t, int64_t, int64_t, int64_t, const std::string&>(), py::arg("num_nodes"),
+             py::arg("hidden") = 64, py::arg("hidden_layers") = 3, py::arg("seed") = 1005,
+             py::arg("device") = std::string("cuda"))
+        .def("Project", &ProposalSampler::Project, py::arg("tree"), py::arg("geo"), py::arg("rays"),
+             py::arg("jitter_seed") = 0)
+        .def("ProjectUniformBinned", &ProposalSampler::ProjectUniformBinned, py::arg("tree"), py::arg("geo"),
+             py::arg("rays"), py::arg("max_samples_per_node"), py::arg("jitter_seed") = 0)
+        .def("ComputeGradients", &ProposalSampler::ComputeGradients, py::arg("tree"))
+        .def("parameters", &ProposalSampler::parameters)
+        .def_readwrite("weight", &ProposalSampler::weight)
+        .def_readwrite("bias", &ProposalSampler::bias)
+        .def_readwrite("occupancy", &ProposalSampler::occupancy)
+        .def_readwrite("budget", &ProposalSampler::budget)
+        .def_readwrite("mass_mix", &ProposalSampler::mass_mix)
+        .def_readwrite("bin_mix", &ProposalSampler::bin_mix)
+        .def_readwrite("mass_weight", &ProposalSampler::mass_weight)
+        .def_readwrite("check_errors", &ProposalSampler::check_errors);
+
     m.def("IndirectGridSample2D", &IndirectGridSample2D);
     m.def("IndirectGridSample1D", &IndirectGridSample1D);
     m.def("GradientCorrection", &GradientCorrection);

@@ -570,6 +570,9 @@ struct ProjectArgs {
     HyperTreeBase* tree;
     int M;
     uint64_t seed;
+    Tensor bins;    // uniform samples: also bin rho * w per segment (optional)
+    Tensor ws;      // workspace to use (required with placed samples)
+    Tensor xt, xw;  // caller-placed samples: t and weight per sample
 };
 
 class ProjectFn : public torch::autograd::Function<ProjectFn> {
@@ -590,17 +593,35 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
         size_t bytes = 0;
         check_status(atdf_project_workspace_size(R, t.max_depth, t.ns, f.num_slots, (int32_t)dims.back(), &bytes),
                      "atdf_project_workspace_size");
-        auto ws = torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
+        const bool placed = a->xt.defined();
+        TORCH_CHECK(!placed || a->ws.defined(), "ProjectRays: placed samples need their workspace");
+        auto ws = a->ws.defined() ? a->ws : torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
+        TORCH_CHECK((size_t)ws.numel() >= bytes, "ProjectRays: workspace too small");
         auto img = torch::empty({dims.back(), R}, o.options());
         auto err = err_word(o.device());
-        check_status(atdf_project_forward(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R, a->M, a->seed,
-                                          img.data_ptr<float>(), ws.data_ptr(), bytes, err.data_ptr<int32_t>(),
-                                          stream_arg()),
-                     "ProjectRays forward");
+        if (placed) {
+            check_status(atdf_project_forward_samples(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R,
+                                                      a->xt.data_ptr<float>(), a->xw.data_ptr<float>(),
+                                                      img.data_ptr<float>(), ws.data_ptr(), (size_t)ws.numel(),
+                                                      err.data_ptr<int32_t>(), stream_arg()),
+                         "ProjectRays forward (placed samples)");
+            ctx->saved_data["xt"] = a->xt;
+            ctx->saved_data["xw"] = a->xw;
+        } else if (a->bins.defined()) {
+            check_status(atdf_project_forward_binned(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R, a->M,
+                                                     a->seed, img.data_ptr<float>(), a->bins.data_ptr<float>(),
+                                                     ws.data_ptr(), (size_t)ws.numel(), err.data_ptr<int32_t>(),
+                                                     stream_arg()),
+                         "ProjectRays forward (binned)");
+        } else {
+            check_status(atdf_project_forward(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R, a->M, a->seed,
+                                              img.data_ptr<float>(), ws.data_ptr(), (size_t)ws.numel(),
+                                              err.data_ptr<int32_t>(), stream_arg()),
+                         "ProjectRays forward");
+        }
         ctx->save_for_backward({o, d, p0, p1, p2, l0, l1, l2, flat});
         ctx->saved_data["ws"] = ws;
         ctx->saved_data["err"] = err;
-        ctx->saved_data["args"] = args_ptr;
         ctx->saved_data["M"] = (int64_t)a->M;
         ctx->saved_data["seed"] = (int64_t)a->seed;
         ctx->saved_data["geo"] = reinterpret_cast<int64_t>(a->geo);
@@ -630,29 +651,43 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
         auto gflat = torch::empty_like(flat);
         auto gmv = mlp_grad_view(dims, gflat.data_ptr<float>());
         auto gi = go[0].contiguous();
-        check_status(atdf_project_backward(&t, &f, &m, s[0].data_ptr<float>(), s[1].data_ptr<float>(), s[0].size(0),
-                                           (int32_t)ctx->saved_data["M"].toInt(),
-                                           (uint64_t)ctx->saved_data["seed"].toInt(), gi.data_ptr<float>(), &gfv, &gmv,
-                                           ws.data_ptr(), (size_t)ws.numel(), err.data_ptr<int32_t>(), stream_arg()),
-                     "ProjectRays backward");
+        if (ctx->saved_data.count("xt")) {
+            auto xt = ctx->saved_data["xt"].toTensor(), xw = ctx->saved_data["xw"].toTensor();
+            check_status(atdf_project_backward_samples(&t, &f, &m, s[0].data_ptr<float>(), s[1].data_ptr<float>(),
+                                                       s[0].size(0), xt.data_ptr<float>(), xw.data_ptr<float>(),
+                                                       gi.data_ptr<float>(), &gfv, &gmv, ws.data_ptr(),
+                                                       (size_t)ws.numel(), err.data_ptr<int32_t>(), stream_arg()),
+                         "ProjectRays backward (placed samples)");
+        } else {
+            check_status(atdf_project_backward(&t, &f, &m, s[0].data_ptr<float>(), s[1].data_ptr<float>(),
+                                               s[0].size(0), (int32_t)ctx->saved_data["M"].toInt(),
+                                               (uint64_t)ctx->saved_data["seed"].toInt(), gi.data_ptr<float>(), &gfv,
+                                               &gmv, ws.data_ptr(), (size_t)ws.numel(), err.data_ptr<int32_t>(),
+                                               stream_arg()),
+                         "ProjectRays backward");
+        }
         return {Tensor(), Tensor(), gp[0], gp[1], gp[2], gl[0], gl[1], gl[2], gflat, Tensor()};
     }
 };
 
-Tensor GeometryTensorQO::ProjectRays(HyperTreeBase& tree, const RayList& rays, int max_samples_per_node,
-                                     uint64_t jitter_seed)
+// The forward reads args only while it runs; the backward uses saved data.
+static Tensor project_apply(GeometryTensorQO& geo, ProjectArgs& args, const RayList& rays)
 {
     ATDF_CHECK_CUDA(rays.origin);
     std::vector<Tensor> P, L;
     for (int m = 0; m < 3; ++m) {
-        P.push_back(channels_last(planes[m]));
-        L.push_back(channels_last(lines[m]));
+        P.push_back(channels_last(geo.planes[m]));
+        L.push_back(channels_last(geo.lines[m]));
     }
-    // the args block lives as long as the autograd node that stores a pointer to it
-    auto holder = std::make_shared<ProjectArgs>(ProjectArgs{this, &tree, max_samples_per_node, jitter_seed});
-    auto img = ProjectFn::apply(rays.origin, rays.direction, P[0], P[1], P[2], L[0], L[1], L[2], flat_params(decoder),
-                                reinterpret_cast<int64_t>(holder.get()));
-    return img;
+    return ProjectFn::apply(rays.origin, rays.direction, P[0], P[1], P[2], L[0], L[1], L[2], flat_params(geo.decoder),
+                            reinterpret_cast<int64_t>(&args));
+}
+
+Tensor GeometryTensorQO::ProjectRays(HyperTreeBase& tree, const RayList& rays, int max_samples_per_node,
+                                     uint64_t jitter_seed)
+{
+    ProjectArgs args{this, &tree, max_samples_per_node, jitter_seed, {}, {}, {}, {}};
+    return project_apply(*this, args, rays);
 }
 
 std::tuple<Tensor, Tensor, Tensor> GeometryTensorQO::ProjectNodeError(HyperTreeBase& tree, const RayList& rays,
@@ -698,6 +733,187 @@ std::tuple<Tensor, Tensor, Tensor> GeometryTensorQO::ProjectNodeError(HyperTreeB
                  "ProjectNodeError");
     check_dev_error(err, "ProjectNodeError");
     return {img, ls, wsum};
+}
+
+// ---------------------------------------------------------------------------
+// Learned proposal sampler
+// ---------------------------------------------------------------------------
+static std::vector<int64_t> proposal_dims(const std::vector<Tensor>& weight)
+{
+    std::vector<int64_t> dims{weight[0].size(1)};
+    for (auto& w : weight) dims.push_back(w.size(0));
+    return dims;
+}
+
+static Tensor proposal_flat(const std::vector<Tensor>& weight, const std::vector<Tensor>& bias)
+{
+    std::vector<Tensor> parts;
+    for (size_t l = 0; l < weight.size(); ++l) {
+        parts.push_back(weight[l].detach().reshape({-1}));
+        parts.push_back(bias[l].detach().reshape({-1}));
+    }
+    return torch::cat(parts).contiguous();
+}
+
+ProposalSampler::ProposalSampler(int64_t num_nodes, int64_t hidden, int64_t hidden_layers, int64_t seed,
+                                 const std::string& device)
+{
+    TORCH_CHECK(hidden == 64 && hidden_layers >= 1 && hidden_layers <= 3,
+                "ProposalSampler: hidden width 64 with 1..3 hidden layers");
+    auto gen = at::make_generator<at::CPUGeneratorImpl>((uint64_t)seed);
+    std::vector<int64_t> dims{ATDF_PROPOSAL_INPUTS};
+    for (int64_t l = 0; l < hidden_layers; ++l) dims.push_back(hidden);
+    dims.push_back(ATDF_PROPOSAL_OUTPUTS);
+    auto opt = torch::TensorOptions().dtype(torch::kFloat32);
+    for (size_t l = 0; l + 1 < dims.size(); ++l) {
+        // torch Linear-style init: Kaiming-normal weights (fan_in), uniform bias
+        auto w = at::normal(0.0, std::sqrt(2.0 / (double)dims[l]), {dims[l + 1], dims[l]}, gen, opt);
+        const double bound = 1.0 / std::sqrt((double)dims[l]);
+        auto b = at::empty({dims[l + 1]}, opt).uniform_(-bound, bound, gen);
+        if (l + 2 == dims.size()) w.mul_(0.1);  // start near the uniform proposal
+        weight.push_back(w.to(torch::Device(device)).set_requires_grad(true));
+        bias.push_back(b.to(torch::Device(device)).set_requires_grad(true));
+    }
+    occupancy = torch::zeros({num_nodes, ATDF_PROPOSAL_OCC}, opt.device(torch::Device(device)));
+}
+
+std::vector<Tensor> ProposalSampler::parameters() const
+{
+    std::vector<Tensor> p;
+    for (size_t l = 0; l < weight.size(); ++l) {
+        p.push_back(weight[l]);
+        p.push_back(bias[l]);
+    }
+    return p;
+}
+
+Tensor ProposalSampler::logits_for(HyperTreeBase& tree, const atdf_segments_t& view, const RayList& rays,
+                                   Tensor* features_out)
+{
+    auto t = tree.view();
+    auto o = rays.origin.contiguous(), d = rays.direction.contiguous();
+    const int64_t cap = std::max<int64_t>(view.capacity, 1);
+    auto feat = torch::empty({cap, ATDF_PROPOSAL_INPUTS}, o.options());
+    auto err = err_word(o.device());
+    TORCH_CHECK(occupancy.size(0) == tree.NumNodes(), "ProposalSampler: occupancy has one row per tree node");
+    check_status(atdf_proposal_features(&t, &view, o.data_ptr<float>(), d.data_ptr<float>(),
+                                        occupancy.data_ptr<float>(), feat.data_ptr<float>(), err.data_ptr<int32_t>(),
+                                        stream_arg()),
+                 "atdf_proposal_features");
+    auto dims = proposal_dims(weight);
+    flat_ = proposal_flat(weight, bias);
+    auto m = mlp_view(dims, flat_.data_ptr<float>(), ATDF_ACT_SILU, ATDF_ACT_ID, 1.0f);
+    auto logits = torch::empty({cap, ATDF_PROPOSAL_OUTPUTS}, o.options());
+    check_status(atdf_proposal_mlp_forward(&m, &view, feat.data_ptr<float>(), logits.data_ptr<float>(), stream_arg()),
+                 "atdf_proposal_mlp_forward");
+    err_ = err;
+    if (features_out) *features_out = feat;
+    return logits;
+}
+
+Tensor ProposalSampler::Project(HyperTreeBase& tree, GeometryTensorQO& geo, const RayList& rays, uint64_t jitter_seed)
+{
+    ATDF_CHECK_CUDA(rays.origin);
+    auto t = tree.view();
+    auto o = rays.origin.contiguous(), d = rays.direction.contiguous();
+    const int64_t R = o.size(0);
+    const int64_t slots = geo.planes[0].size(0);
+    size_t bytes = 0;
+    check_status(atdf_project_workspace_size(R, t.max_depth, t.ns, slots, 1, &bytes), "atdf_project_workspace_size");
+    auto ws = torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
+    auto err = err_word(o.device());
+    atdf_segments_t view;
+    check_status(atdf_project_segments(&t, o.data_ptr<float>(), d.data_ptr<float>(), R, 1, slots, ws.data_ptr(), bytes,
+                                       &view, err.data_ptr<int32_t>(), stream_arg()),
+                 "atdf_project_segments");
+    auto logits = logits_for(tree, view, rays, nullptr);
+    check_status(atdf_proposal_allocate(&view, R, logits.data_ptr<float>(), (int32_t)budget, (float)mass_mix,
+                                        stream_arg()),
+                 "atdf_proposal_allocate");
+    // a ray gets at most max(budget, its segment count) samples: no host read needed
+    const int64_t cap = R * budget + view.capacity;
+    auto xt = torch::empty({std::max<int64_t>(cap, 1)}, o.options());
+    auto xw = torch::empty_like(xt);
+    check_status(atdf_proposal_samples(&view, logits.data_ptr<float>(), (float)bin_mix, jitter_seed,
+                                       xt.data_ptr<float>(), xw.data_ptr<float>(), cap, err.data_ptr<int32_t>(),
+                                       stream_arg()),
+                 "atdf_proposal_samples");
+    ProjectArgs args{&geo, &tree, 0, 0, {}, ws, xt, xw};
+    auto img = project_apply(geo, args, rays);
+    if (check_errors) {
+        check_dev_error(err, "ProposalSampler::Project");
+        check_dev_error(err_, "atdf_proposal_features");
+    }
+    return img;
+}
+
+Tensor ProposalSampler::ProjectUniformBinned(HyperTreeBase& tree, GeometryTensorQO& geo, const RayList& rays,
+                                             int max_samples_per_node, uint64_t jitter_seed)
+{
+    ATDF_CHECK_CUDA(rays.origin);
+    auto t = tree.view();
+    const int64_t R = rays.origin.size(0);
+    const int64_t slots = geo.planes[0].size(0);
+    size_t bytes = 0;
+    check_status(atdf_project_workspace_size(R, t.max_depth, t.ns, slots, 1, &bytes), "atdf_project_workspace_size");
+    auto ws = torch::empty({(int64_t)bytes}, rays.origin.options().dtype(torch::kUInt8));
+    atdf_segments_t view;
+    check_status(atdf_project_segment_view(R, t.max_depth, slots, ws.data_ptr(), bytes, &view),
+                 "atdf_project_segment_view");
+    // bins [segment capacity][32], indexed like the workspace's segment arrays
+    auto bins = torch::empty({view.capacity, ATDF_PROPOSAL_BINS}, rays.origin.options());
+    ProjectArgs args{&geo, &tree, max_samples_per_node, jitter_seed, bins, ws, {}, {}};
+    auto img = project_apply(geo, args, rays);
+    last_ws_ = ws;
+    last_bins_ = bins;
+    last_rays_ = RayList{rays.origin.contiguous(), rays.direction.contiguous()};
+    last_slots_ = slots;
+    return img;
+}
+
+Tensor ProposalSampler::ComputeGradients(HyperTreeBase& tree)
+{
+    TORCH_CHECK(last_ws_.defined(), "ProposalSampler::ComputeGradients: run ProjectUniformBinned first");
+    torch::NoGradGuard ng;
+    auto t = tree.view();
+    const int64_t R = last_rays_.origin.size(0);
+    atdf_segments_t view;
+    check_status(atdf_project_segment_view(R, t.max_depth, last_slots_, last_ws_.data_ptr(),
+                                           (size_t)last_ws_.numel(), &view),
+                 "atdf_project_segment_view");
+    Tensor feat;
+    auto logits = logits_for(tree, view, last_rays_, &feat);
+    const int64_t nn = tree.NumNodes();
+    auto dopt = last_bins_.options().dtype(torch::kFloat64);
+    auto loss = torch::empty({}, dopt);
+    auto node_mass = torch::empty({nn, ATDF_PROPOSAL_OCC}, dopt), node_len = torch::empty({nn, ATDF_PROPOSAL_OCC}, dopt);
+    auto dlogits = torch::empty_like(logits);
+    auto err = err_word(last_ws_.device());
+    check_status(atdf_proposal_loss(&view, feat.data_ptr<float>(), last_bins_.data_ptr<float>(),
+                                    logits.data_ptr<float>(), (float)mass_weight, dlogits.data_ptr<float>(),
+                                    loss.data_ptr<double>(), node_mass.data_ptr<double>(), node_len.data_ptr<double>(),
+                                    nn, err.data_ptr<int32_t>(), stream_arg()),
+                 "atdf_proposal_loss");
+    auto dims = proposal_dims(weight);
+    auto m = mlp_view(dims, flat_.data_ptr<float>(), ATDF_ACT_SILU, ATDF_ACT_ID, 1.0f);
+    auto gflat = torch::empty_like(flat_);
+    auto gm = mlp_grad_view(dims, gflat.data_ptr<float>());
+    check_status(atdf_proposal_mlp_backward(&m, &view, feat.data_ptr<float>(), dlogits.data_ptr<float>(), &gm,
+                                            stream_arg()),
+                 "atdf_proposal_mlp_backward");
+    int64_t off = 0;
+    for (size_t l = 0; l < weight.size(); ++l) {
+        const int64_t nw = weight[l].numel(), nb = bias[l].numel();
+        weight[l].mutable_grad() = gflat.slice(0, off, off + nw).view(weight[l].sizes());
+        off += nw;
+        bias[l].mutable_grad() = gflat.slice(0, off, off + nb);
+        off += nb;
+    }
+    check_status(atdf_proposal_occupancy(node_mass.data_ptr<double>(), node_len.data_ptr<double>(), nn,
+                                         occupancy.data_ptr<float>(), stream_arg()),
+                 "atdf_proposal_occupancy");
+    if (check_errors) check_dev_error(err, "atdf_proposal_loss");
+    return loss;
 }
 
 }  // namespace atdf_host

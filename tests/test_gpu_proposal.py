@@ -1,0 +1,428 @@
+"""Learned proposal sampler on the GPU: projections with caller-placed
+samples against the oracle, the binned forward, the proposal kernels against
+their restatement (numpy for the sampler, the C++ oracle for the MLP),
+unbiasedness, and the gain of a trained proposal over uniform sampling."""
+
+import ctypes as ct
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import proposal_oracle as po
+from scene import gpu_scene, oracle_views, rel_err
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-5
+
+
+def _rays(o, d):
+    import adaptivetensordf_b200 as ab
+
+    return ab.RayList(torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda())
+
+
+def _dev(ws, addr, n, dtype):
+    """Device array inside the workspace tensor at address addr."""
+    item = torch.empty((), dtype=dtype).element_size()
+    off = addr - ws.data_ptr()
+    return ws[off:off + n * item].view(dtype)
+
+
+class Placed:
+    """Segments of a ray batch in a fused workspace, through the C ABI."""
+
+    def __init__(self, tree, geo, o, d, M):
+        from adaptivetensordf_b200 import capi
+
+        self.L = capi.lib()
+        self.capi = capi
+        self.tree, self.geo = tree, geo
+        self.o = torch.from_numpy(o).cuda()
+        self.d = torch.from_numpy(d).cuda()
+        self.R = o.shape[0]
+        self.ts = capi.tree_struct(tree)
+        self.slots = geo.planes[0].shape[0]
+        nb = ct.c_size_t()
+        assert self.L.atdf_project_workspace_size(self.R, tree.max_depth, tree.NS(), self.slots, 1,
+                                                  ct.byref(nb)) == 0
+        self.ws = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+        self.view = capi.Segments()
+        self.err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        st = self.L.atdf_project_segments(ct.byref(self.ts), capi.ptr(self.o), capi.ptr(self.d), self.R, M,
+                                          self.slots, capi.ptr(self.ws), self.ws.numel(), ct.byref(self.view),
+                                          capi.ptr(self.err), None)
+        assert st == 0
+        torch.cuda.synchronize()
+        assert int(self.err.item()) == 0
+
+    def totals(self):
+        return _dev(self.ws, self.view.totals, 4, torch.int64).cpu().numpy()
+
+    def arrays(self):
+        G = int(self.totals()[0])
+        v, ws, R = self.view, self.ws, self.R
+        return {
+            "node": _dev(ws, v.node, G, torch.int32).cpu().numpy(),
+            "tmin": _dev(ws, v.tmin, G, torch.float32).cpu().numpy(),
+            "tmax": _dev(ws, v.tmax, G, torch.float32).cpu().numpy(),
+            "n": _dev(ws, v.nsamp, G, torch.int32).cpu().numpy(),
+            "ray": _dev(ws, v.ray, G, torch.int32).cpu().numpy(),
+            "first": _dev(ws, v.first, G, torch.int32).cpu().numpy(),
+            "ray_seg_offset": _dev(ws, v.ray_seg_offset, R + 1, torch.int64).cpu().numpy(),
+            "ray_sample_offset": _dev(ws, v.ray_sample_offset, R + 1, torch.int64).cpu().numpy(),
+        }
+
+    def forward(self, xt, xw):
+        c = self.capi
+        fs, keep = c.field_struct(self.geo)
+        ms, keep2 = c.mlp_struct(self.geo)
+        img = torch.empty(1, self.R, device="cuda")
+        st = self.L.atdf_project_forward_samples(ct.byref(self.ts), ct.byref(fs), ct.byref(ms), c.ptr(self.o),
+                                                 c.ptr(self.d), self.R, c.ptr(xt), c.ptr(xw), c.ptr(img),
+                                                 c.ptr(self.ws), self.ws.numel(), c.ptr(self.err), None)
+        assert st == 0
+        torch.cuda.synchronize()
+        return img
+
+    def backward(self, xt, xw, gi):
+        c = self.capi
+        fs, keep = c.field_struct(self.geo)
+        ms, keep2 = c.mlp_struct(self.geo)
+        gp = [torch.empty_like(p.detach().contiguous(memory_format=torch.channels_last)) for p in self.geo.planes]
+        gl = [torch.empty_like(ln.detach().contiguous(memory_format=torch.channels_last)) for ln in self.geo.lines]
+        gw = [torch.empty_like(w.detach()) for w in self.geo.decoder_weight]
+        gb = [torch.empty_like(b.detach()) for b in self.geo.decoder_bias]
+        fg = c.FieldGrad()
+        for m in range(3):
+            fg.plane[m] = gp[m].data_ptr()
+            fg.line[m] = gl[m].data_ptr()
+        mg = c.MlpGrad()
+        for i in range(len(gw)):
+            mg.weight[i] = gw[i].data_ptr()
+            mg.bias[i] = gb[i].data_ptr()
+        st = self.L.atdf_project_backward_samples(ct.byref(self.ts), ct.byref(fs), ct.byref(ms), c.ptr(self.o),
+                                                  c.ptr(self.d), self.R, c.ptr(xt), c.ptr(xw), c.ptr(gi),
+                                                  ct.byref(fg), ct.byref(mg), c.ptr(self.ws), self.ws.numel(),
+                                                  c.ptr(self.err), None)
+        assert st == 0
+        torch.cuda.synchronize()
+        return gp, gl, gw, gb
+
+
+def _samples_from_t(o, d, segs, t, w):
+    """Oracle SampleList for placed samples (t, w in canonical order)."""
+    ray = np.repeat(segs["ray"].astype(np.int64), segs["n"])
+    node = np.repeat(segs["node"].astype(np.int64), segs["n"])
+    t32 = t.astype(np.float32)
+    pos = (o[ray] + (d[ray] * t32[:, None]).astype(np.float32)).astype(np.float32)
+    return {"global_coordinate": pos, "ray_t": t32, "weight": w.astype(np.float32), "ray_index": ray,
+            "node_id": node}
+
+
+def _check_grads(gp, gl, gw, gb, gr):
+    for m in range(3):
+        assert rel_err(gp[m].cpu().numpy(), gr["planes"][m]) < REL_TOL, f"plane {m}"
+        assert rel_err(gl[m].cpu().numpy(), gr["lines"][m]) < REL_TOL, f"line {m}"
+    for i in range(len(gw)):
+        assert rel_err(gw[i].cpu().numpy(), gr["W"][i]) < REL_TOL, f"W{i}"
+        assert rel_err(gb[i].cpu().numpy(), gr["b"][i]) < REL_TOL, f"b{i}"
+
+
+def test_placed_uniform_samples_match_oracle(oracle):
+    """Caller-placed samples equal to the uniform sampler's reproduce the
+    oracle's projection and adjoint."""
+    R, M, seed = 600, 16, 77
+    tree, geo, o, d = gpu_scene(2, 8, 17, (64, 17, 64), [32], R, seed=4)
+    td, fd, md = oracle_views(tree, geo)
+    pl = Placed(tree, geo, o, d, M)
+    a = pl.arrays()
+    segs_o = oracle.ray_segments(td, o, d, M)
+    for k in ("node", "tmin", "tmax", "n", "ray"):
+        assert np.array_equal(a[k], segs_o[k]), k
+    so = oracle.emit_samples(segs_o, o, d, oracle.jitter_for_segments(seed, segs_o))
+    xt = torch.from_numpy(so["ray_t"]).cuda()
+    xw = torch.from_numpy(so["weight"]).cuda()
+    img = pl.forward(xt, xw)
+    img_o = oracle.project_forward(fd, md, td, so, R, np.float64)
+    assert rel_err(img.cpu().numpy(), img_o) < REL_TOL
+    gi = np.random.default_rng(2).normal(size=img_o.shape)
+    res = pl.backward(xt, xw, torch.from_numpy(gi.astype(np.float32)).cuda())
+    _check_grads(*res, oracle.project_backward(fd, md, td, so, R, gi, np.float64))
+
+
+def test_placed_arbitrary_samples_match_oracle(oracle):
+    """Non-uniform placed samples (the proposal's own t and w) through the
+    FP32 fused kernels vs the oracle on the same samples."""
+    R = 500
+    tree, geo, o, d = gpu_scene(3, 16, 17, (128, 17, 128), [64, 64], R, seed=5)
+    td, fd, md = oracle_views(tree, geo)
+    pl = Placed(tree, geo, o, d, 1)
+    logits = torch.randn(pl.view.capacity, po.OUTPUTS, device="cuda") * 1.5
+    L, c = pl.L, pl.capi
+    assert L.atdf_proposal_allocate(ct.byref(pl.view), R, c.ptr(logits), 48, ct.c_float(0.25), None) == 0
+    S = int(pl.totals()[1])
+    xt = torch.empty(S, device="cuda")
+    xw = torch.empty(S, device="cuda")
+    assert L.atdf_proposal_samples(ct.byref(pl.view), c.ptr(logits), ct.c_float(0.2), 99, c.ptr(xt), c.ptr(xw), S,
+                                   c.ptr(pl.err), None) == 0
+    torch.cuda.synchronize()
+    assert int(pl.err.item()) == 0
+    so = _samples_from_t(o, d, pl.arrays(), xt.cpu().numpy(), xw.cpu().numpy())
+    img = pl.forward(xt, xw)
+    img_o = oracle.project_forward(fd, md, td, so, R, np.float64)
+    assert rel_err(img.cpu().numpy(), img_o) < REL_TOL
+    gi = np.random.default_rng(3).normal(size=img_o.shape)
+    res = pl.backward(xt, xw, torch.from_numpy(gi.astype(np.float32)).cuda())
+    _check_grads(*res, oracle.project_backward(fd, md, td, so, R, gi, np.float64))
+
+
+def test_binned_forward_sums_to_image(oracle):
+    """Bins of rho * w: their per-ray sums are the image, and each bin holds
+    exactly the oracle samples whose t falls in it."""
+    from adaptivetensordf_b200 import capi
+
+    R, M, seed = 400, 12, 5
+    tree, geo, o, d = gpu_scene(2, 8, 17, (64, 17, 64), [32], R, seed=6)
+    td, fd, md = oracle_views(tree, geo)
+    L = capi.lib()
+    pl = Placed(tree, geo, o, d, M)
+    bins = torch.empty(pl.view.capacity, po.BINS, device="cuda")
+    img = torch.empty(1, R, device="cuda")
+    fs, k1 = capi.field_struct(geo)
+    ms, k2 = capi.mlp_struct(geo)
+    st = L.atdf_project_forward_binned(ct.byref(pl.ts), ct.byref(fs), ct.byref(ms), capi.ptr(pl.o), capi.ptr(pl.d), R,
+                                       M, seed, capi.ptr(img), capi.ptr(bins), capi.ptr(pl.ws), pl.ws.numel(),
+                                       capi.ptr(pl.err), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    a = pl.arrays()
+    G = len(a["node"])
+    b = bins[:G].double().cpu().numpy()
+    per_ray = np.zeros(R)
+    np.add.at(per_ray, a["ray"], b.sum(1))
+    assert rel_err(per_ray, img.cpu().numpy()[0]) < REL_TOL
+    segs_o = oracle.ray_segments(td, o, d, M)
+    so = oracle.emit_samples(segs_o, o, d, oracle.jitter_for_segments(seed, segs_o))
+    feat = oracle.vm_features(fd, td, so["global_coordinate"], so["node_id"], np.float64)
+    rho = oracle.mlp_forward(md, feat, np.float64)[:, 0]
+    seg = np.repeat(np.arange(G), segs_o["n"])
+    t = so["ray_t"]
+    tmin = segs_o["tmin"][seg]
+    ln = (segs_o["tmax"] - segs_o["tmin"])[seg]
+    bi = np.clip(((t - tmin) / ln * np.float32(32)).astype(np.float32).astype(np.int64), 0, 31)
+    ref = np.zeros((G, po.BINS))
+    np.add.at(ref, (seg, bi), rho * so["weight"])
+    assert rel_err(b, ref) < 1e-5
+
+
+def test_proposal_kernels_match_restatement(oracle):
+    R = 300
+    tree, geo, o, d = gpu_scene(3, 8, 9, (64, 9, 64), [32], R, seed=8)
+    pl = Placed(tree, geo, o, d, 1)
+    L, c = pl.L, pl.capi
+    a = pl.arrays()
+    G = len(a["node"])
+    nn = tree.NumNodes()
+    nmin = tree.node_position_min.cpu().numpy()
+    nmax = tree.node_position_max.cpu().numpy()
+    occ = torch.rand(nn, po.OCC, device="cuda")
+    feat = torch.zeros(pl.view.capacity, po.INPUTS, device="cuda")
+    assert L.atdf_proposal_features(ct.byref(pl.ts), ct.byref(pl.view), c.ptr(pl.o), c.ptr(pl.d), c.ptr(occ),
+                                    c.ptr(feat), c.ptr(pl.err), None) == 0
+    f_ref = po.features(nmin, nmax, o, d, a["node"], a["ray"], a["tmin"], a["tmax"], occ.cpu().numpy())
+    assert np.abs(feat[:G].cpu().numpy() - f_ref).max() < 1e-4
+    logits = torch.randn(pl.view.capacity, po.OUTPUTS, device="cuda") * 2
+    lg = logits.cpu().numpy().astype(np.float64)
+    budget = 40
+    assert L.atdf_proposal_allocate(ct.byref(pl.view), R, c.ptr(logits), budget, ct.c_float(0.3), None) == 0
+    b = pl.arrays()
+    n_ref, first_ref, off_ref = po.allocate(a["ray_seg_offset"], a["tmin"], a["tmax"], lg, budget, 0.3)
+    diff = b["n"].astype(np.int64) - n_ref
+    assert np.abs(diff).max() <= 1 and (diff != 0).mean() < 0.01
+    seg_count = np.diff(a["ray_seg_offset"])
+    per_ray = np.diff(b["ray_sample_offset"])
+    assert np.all(per_ray <= np.maximum(budget, seg_count)) and np.all(per_ray >= seg_count)
+    assert np.all(b["n"] >= 1)
+    S = int(pl.totals()[1])
+    assert S == int(b["ray_sample_offset"][-1])
+    for seed in (0, 4242):
+        xt = torch.empty(S, device="cuda")
+        xw = torch.empty(S, device="cuda")
+        assert L.atdf_proposal_samples(ct.byref(pl.view), c.ptr(logits), ct.c_float(0.2), seed, c.ptr(xt),
+                                       c.ptr(xw), S, c.ptr(pl.err), None) == 0
+        torch.cuda.synchronize()
+        jit = None
+        if seed:
+            jit = [[oracle.jitter(seed, int(b["ray"][s]), int(b["node"][s]), j) for j in range(int(b["n"][s]))]
+                   for s in range(G)]
+        t_ref, w_ref = po.samples(b["tmin"], b["tmax"], b["n"], lg, 0.2, jit)
+        t = xt.cpu().numpy()
+        w = xw.cpu().numpy()
+        ln = np.repeat(b["tmax"] - b["tmin"], b["n"])
+        assert np.abs(t - t_ref).max() <= 1e-4 * max(1.0, ln.max())
+        assert rel_err(w, w_ref) < 1e-4
+        seg = np.repeat(np.arange(G), b["n"])
+        assert np.all(t >= b["tmin"][seg]) and np.all(t <= b["tmax"][seg])
+    # loss, its gradient, and the occupancy sums
+    rng = np.random.default_rng(1)
+    hb = rng.gamma(0.3, 1.0, (G, po.BINS)).astype(np.float32)
+    hb[::7] = 0.0
+    bins = torch.zeros(pl.view.capacity, po.BINS, device="cuda")
+    bins[:G] = torch.from_numpy(hb).cuda()
+    dl = torch.zeros_like(logits)
+    loss = torch.zeros((), dtype=torch.float64, device="cuda")
+    nm = torch.zeros(nn, po.OCC, dtype=torch.float64, device="cuda")
+    nl = torch.zeros_like(nm)
+    assert L.atdf_proposal_loss(ct.byref(pl.view), c.ptr(feat), c.ptr(bins), c.ptr(logits), ct.c_float(0.1),
+                                c.ptr(dl), c.ptr(loss), c.ptr(nm), c.ptr(nl), nn, c.ptr(pl.err), None) == 0
+    torch.cuda.synchronize()
+    length = (b["tmax"] - b["tmin"]).astype(np.float64)
+    L_ref, d_ref, m_ref = po.loss(hb, lg, length, 0.1)
+    assert abs(float(loss.item()) - L_ref) < 1e-4 * abs(L_ref)
+    assert rel_err(dl[:G].cpu().numpy(), d_ref) < 1e-4
+    nm_ref, nl_ref = po.node_occupancy_sums(hb, feat[:G].cpu().numpy().astype(np.float64), length, b["node"], nn)
+    assert rel_err(nm.cpu().numpy()[:, 8], nm_ref[:, 8]) < 1e-6
+    assert rel_err(nl.cpu().numpy()[:, 8], nl_ref[:, 8]) < 1e-6
+    # octant sums: a bin centre exactly on an octant plane may round either way
+    assert rel_err(nm.cpu().numpy()[:, :8], nm_ref[:, :8]) < 1e-3
+    occ_before = occ.clone()
+    assert L.atdf_proposal_occupancy(c.ptr(nm), c.ptr(nl), nn, c.ptr(occ), None) == 0
+    torch.cuda.synchronize()
+    nl_c = nl.cpu().numpy()
+    exp = np.where(nl_c > 0, nm.cpu().numpy() / np.where(nl_c > 0, nl_c, 1), occ_before.cpu().numpy())
+    assert np.allclose(occ.cpu().numpy(), exp, rtol=1e-6, atol=0)
+    assert int(pl.err.item()) == 0
+
+
+@pytest.mark.parametrize("hidden_layers", [1, 3])
+def test_proposal_mlp_kernels_match_oracle(oracle, hidden_layers):
+    """The proposal network (16 -> 64 x n -> 33, SiLU) forward and weight
+    gradients from the tiled proposal-MLP kernels vs the oracle's MLP, over
+    a row count read on the device."""
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import capi
+
+    R = 700
+    tree, geo, o, d = gpu_scene(3, 8, 9, (64, 9, 64), [32], R, seed=2)
+    pl = Placed(tree, geo, o, d, 1)
+    G = int(pl.totals()[0])
+    ps = ab.ProposalSampler(tree.NumNodes(), 64, hidden_layers, 7, "cuda")
+    x = np.random.default_rng(0).normal(size=(pl.view.capacity, po.INPUTS)).astype(np.float32)
+    md = {"layers": [(w.detach().cpu().numpy(), b.detach().cpu().numpy()) for w, b in zip(ps.weight, ps.bias)],
+          "act": "silu", "last_act": "id", "beta": 1.0}
+    L = capi.lib()
+    m = capi.Mlp()
+    ws = [w.detach().contiguous() for w in ps.weight]
+    bs = [b.detach().contiguous() for b in ps.bias]
+    m.num_layers = len(ws)
+    m.dims[0] = po.INPUTS
+    for i, w in enumerate(ws):
+        m.dims[i + 1] = w.shape[0]
+        m.weight[i] = w.data_ptr()
+        m.bias[i] = bs[i].data_ptr()
+    m.hidden_activation = capi.ACT["silu"]
+    m.last_activation = capi.ACT["id"]
+    m.softplus_beta = 1.0
+    xd = torch.from_numpy(x).cuda()
+    out = torch.full((pl.view.capacity, po.OUTPUTS), 7.0, device="cuda")
+    assert L.atdf_proposal_mlp_forward(ct.byref(m), ct.byref(pl.view), capi.ptr(xd), capi.ptr(out), None) == 0
+    torch.cuda.synchronize()
+    ref = oracle.mlp_forward(md, x[:G], np.float64)
+    assert rel_err(out[:G].cpu().numpy(), ref) < REL_TOL
+    assert torch.all(out[G:] == 7.0)  # rows past the segment count are untouched
+    g = np.random.default_rng(1).normal(size=(pl.view.capacity, po.OUTPUTS))
+    gw = [torch.full_like(w, 3.0) for w in ws]  # overwritten by the call
+    gb = [torch.full_like(b, 3.0) for b in bs]
+    mg = capi.MlpGrad()
+    for i in range(len(ws)):
+        mg.weight[i] = gw[i].data_ptr()
+        mg.bias[i] = gb[i].data_ptr()
+    gd = torch.from_numpy(g.astype(np.float32)).cuda()
+    assert L.atdf_proposal_mlp_backward(ct.byref(m), ct.byref(pl.view), capi.ptr(xd), capi.ptr(gd), ct.byref(mg),
+                                        None) == 0
+    torch.cuda.synchronize()
+    dW, db, _ = oracle.mlp_backward(md, x[:G], g[:G], np.float64)
+    for i in range(len(ws)):
+        assert rel_err(gw[i].cpu().numpy(), dW[i]) < REL_TOL, i
+        assert rel_err(gb[i].cpu().numpy(), db[i]) < REL_TOL, i
+
+
+def test_proposal_projection_is_unbiased():
+    """The mean over jitter seeds of projections through a random (untrained)
+    proposal converges to the dense uniform projection at the Monte Carlo
+    rate: its error is that of one projection divided by about sqrt(K)."""
+    import adaptivetensordf_b200 as ab
+
+    R = 256
+    tree, geo, o, d = gpu_scene(2, 8, 17, (64, 17, 64), [32], R, seed=12)
+    rays = _rays(o, d)
+    ps = ab.ProposalSampler(tree.NumNodes(), 64, 3, 3, "cuda")
+    ps.check_errors = True
+    with torch.no_grad():
+        ps.weight[-1].normal_(0, 0.3)
+        ps.bias[-1].normal_(0, 1.0)
+        ps.occupancy.uniform_(0, 1)
+        ps.budget = 24
+        dense = geo.ProjectRays(tree, rays, 512, 0).double()
+        K = 256
+        acc = torch.zeros_like(dense)
+        singles = []
+        for k in range(K):
+            one = ps.Project(tree, geo, rays, 1000 + k).double()
+            acc += one
+            if k < 16:
+                singles.append(float((one - dense).norm() / dense.norm()))
+        mean = acc / K
+    e_mean = float((mean - dense).norm() / dense.norm())
+    e_one = float(np.sqrt(np.mean(np.square(singles))))
+    print(f"single projection error {e_one:.3e}, mean of {K}: {e_mean:.3e}")
+    assert e_mean < 2.5 * e_one / np.sqrt(K) + 2e-5, (e_mean, e_one)
+
+
+def test_trained_proposal_beats_uniform_sampling():
+    """After online training on uniform passes of a fitted field, projections
+    through the proposal at a budget of 64 samples per ray have a smaller
+    error than uniform per-node sampling with at least as many samples."""
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import recon
+    from adaptivetensordf_b200 import synthetic as syn
+
+    cfg = syn.CONFIGS["C1"]
+    data = recon.make_tilt_series(cfg)
+    opt = recon.TrainOptions(epochs=8, batch=4096, max_samples_per_node=cfg.max_samples_per_node,
+                             stop_at_target=False, init_scale=0.05)
+    tree, geo = recon.build_model(cfg, "fp32", init_scale=0.05)
+    recon.fit(tree, geo, data, opt)
+    ps = ab.ProposalSampler(tree.NumNodes(), 64, 3, 1005, "cuda")
+    ps.budget = 64
+    adam = torch.optim.Adam(ps.parameters(), lr=3e-3)
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    losses = []
+    for it in range(300):
+        idx = torch.randint(0, data.num_rays, (4096,), device="cuda", generator=gen)
+        rays = ab.RayList(data.origin[idx], data.direction[idx])
+        with torch.no_grad():
+            ps.ProjectUniformBinned(tree, geo, rays, cfg.max_samples_per_node, it + 1)
+        adam.zero_grad()
+        losses.append(ps.ComputeGradients(tree))
+        adam.step()
+    losses = [float(x) for x in losses]
+    idx = torch.randint(0, data.num_rays, (8192,), device="cuda", generator=gen)
+    rays = ab.RayList(data.origin[idx], data.direction[idx])
+    with torch.no_grad():
+        dense = geo.ProjectRays(tree, rays, 1024, 0).double()
+        e_prop = np.mean([float((ps.Project(tree, geo, rays, 31 + k).double() - dense).norm() / dense.norm())
+                          for k in range(4)])
+        M = 16
+        while tree.CreateSamplesForRays(rays, M, False).size() / 8192 < 64:
+            M += 2
+        n_uni = tree.CreateSamplesForRays(rays, M, False).size() / 8192
+        e_uni = np.mean([float((geo.ProjectRays(tree, rays, M, 31 + k).double() - dense).norm() / dense.norm())
+                         for k in range(4)])
+    print(f"proposal loss {losses[0]:.3f} -> {losses[-1]:.3f}; proposal error {e_prop:.3e} at <= 64 samples/ray; "
+          f"uniform {e_uni:.3e} at {n_uni:.1f} samples/ray (M = {M})")
+    assert losses[-1] < losses[0]
+    assert n_uni >= 64
+    assert e_prop < e_uni
