@@ -3,9 +3,10 @@
 // segment's mass, from the segment's leaf-local entry and exit points, its
 // relative length and the leaf's occupancy (whole leaf and 8 octants). A
 // ray's sample budget is split over its segments by predicted mass, and each
-// segment's samples are drawn by stratified inverse-CDF sampling of its bin
-// density and weighted by 1 / (n q(t)), so the line integral stays unbiased
-// for any proposal. The network is trained on the bins of rho * w that the
+// segment's samples are placed by stratified inverse-CDF sampling of its bin
+// density and weighted by their Voronoi cells along the segment, the
+// quadrature the uniform sampler uses (HyperTree.cu:495-512), so dense
+// placement refines the quadrature where the density is. The network is trained on the bins of rho * w that the
 // uniform sampler's forward pass produces (atdf_project_forward_binned), and
 // those bins also refresh the occupancy.
 //
@@ -341,11 +342,18 @@ __global__ void __launch_bounds__(kPThreads, 1) proposal_mlp_bwd_kernel(PropMlp 
 // ---------------------------------------------------------------------------
 // allocation, sampling, loss, occupancy
 // ---------------------------------------------------------------------------
+// Allocation weight of a segment: len * (predicted mean density)^power.
+__device__ __forceinline__ float alloc_weight(const float* lg, float len, float power)
+{
+    const float dens = softplus1(lg[kPropBins]);
+    return power == 0.0f ? len : len * __powf(fmaxf(dens, 1e-20f), power);
+}
+
 // One thread per ray: sample counts of the ray's segments from the predicted
-// masses; writes nsamp, first (within the ray) and the ray's total into
+// densities; writes nsamp, first (within the ray) and the ray's total into
 // ray_sample_offset[r] (scanned afterwards).
 __global__ void proposal_allocate_kernel(atdf_segments_t segs, int64_t R, const float* __restrict__ logits,
-                                         int32_t budget, float mass_mix)
+                                         int32_t budget, float mass_mix, float mass_power)
 {
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
@@ -354,17 +362,17 @@ __global__ void proposal_allocate_kernel(atdf_segments_t segs, int64_t R, const 
     float msum = 0.0f, lsum = 0.0f;
     for (int64_t s = b; s < e; ++s) {
         const float len = segs.tmax[s] - segs.tmin[s];
-        msum += softplus1(logits[s * kPropOut + kPropBins]) * len;
+        msum += alloc_weight(logits + s * kPropOut, len, mass_power);
         lsum += len;
     }
     const int spare = budget > nseg ? budget - nseg : 0;
     int run = 0;
     for (int64_t s = b; s < e; ++s) {
         const float len = segs.tmax[s] - segs.tmin[s];
-        const float m = softplus1(logits[s * kPropOut + kPropBins]) * len;
+        const float m = alloc_weight(logits + s * kPropOut, len, mass_power);
         float share = lsum > 0.0f ? len / lsum : 1.0f / (float)nseg;
         if (msum > 0.0f) share = (1.0f - mass_mix) * (m / msum) + mass_mix * share;
-        const int n = 1 + (int)floorf((float)spare * share);
+        const int n = 1 + (int)floorf((float)spare * share + 0.5f);
         segs.nsamp[s] = n;
         segs.first[s] = run;
         run += n;
@@ -373,15 +381,16 @@ __global__ void proposal_allocate_kernel(atdf_segments_t segs, int64_t R, const 
     atomicMax((unsigned long long*)&segs.totals[2], (unsigned long long)run);
 }
 
-// Bin probabilities of a segment: softmax of the 32 logits mixed with the
-// uniform density.
-__device__ __forceinline__ void bin_probs(const float* lg, float bin_mix, float* p)
+// Bin probabilities of a segment: softmax of power * (the 32 logits), i.e.
+// the predicted bin distribution raised to power and renormalised, mixed
+// with the uniform density.
+__device__ __forceinline__ void bin_probs(const float* lg, float bin_mix, float* p, float power = 1.0f)
 {
     float mx = lg[0];
     for (int b = 1; b < kPropBins; ++b) mx = fmaxf(mx, lg[b]);
     float sum = 0.0f;
     for (int b = 0; b < kPropBins; ++b) {
-        p[b] = __expf(lg[b] - mx);
+        p[b] = __expf(power * (lg[b] - mx));
         sum += p[b];
     }
     const float inv = (1.0f - bin_mix) / sum, u = bin_mix / (float)kPropBins;
@@ -389,8 +398,8 @@ __device__ __forceinline__ void bin_probs(const float* lg, float bin_mix, float*
 }
 
 __global__ void proposal_samples_kernel(atdf_segments_t segs, const float* __restrict__ logits, float bin_mix,
-                                        uint64_t seed, float* __restrict__ sample_t, float* __restrict__ sample_w,
-                                        int64_t capacity, int32_t* err)
+                                        float bin_power, uint64_t seed, float* __restrict__ sample_t,
+                                        float* __restrict__ sample_w, int64_t capacity, int32_t* err)
 {
     const int64_t nseg = segs.totals[0];
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += (int64_t)gridDim.x * blockDim.x) {
@@ -402,12 +411,13 @@ __global__ void proposal_samples_kernel(atdf_segments_t segs, const float* __res
             continue;
         }
         float p[kPropBins];
-        bin_probs(logits + s * kPropOut, bin_mix, p);
+        bin_probs(logits + s * kPropOut, bin_mix, p, bin_power);
         const float t0 = segs.tmin[s], t1 = segs.tmax[s];
         const float binw = (t1 - t0) / (float)kPropBins;
         int bcur = 0;
         float cdf = 0.0f;  // CDF at the start of bin bcur
-        for (int j = 0; j < n; ++j) {
+        // t of sample j; j increases, so the bin search only moves forward
+        auto place = [&](int j) {
             const float a = seed ? jitter(seed, r, node, j) : 0.5f;
             const float u = ((float)j + a) / (float)n;
             while (bcur < kPropBins - 1 && cdf + p[bcur] <= u) {
@@ -416,10 +426,18 @@ __global__ void proposal_samples_kernel(atdf_segments_t segs, const float* __res
             }
             float frac = (u - cdf) / p[bcur];
             frac = fminf(fmaxf(frac, 0.0f), 1.0f);
-            float t = t0 + ((float)bcur + frac) * binw;
-            t = fminf(fmaxf(t, t0), t1);
-            sample_t[base + j] = t;
-            sample_w[base + j] = binw / ((float)n * p[bcur]);
+            const float t = t0 + ((float)bcur + frac) * binw;
+            return fminf(fmaxf(t, t0), t1);
+        };
+        // weights: the Voronoi cells of the placed samples within the segment,
+        // the rule the uniform sampler applies to its own samples
+        float t_prev = 0.0f, t_cur = place(0);
+        for (int j = 0; j < n; ++j) {
+            const float t_next = j + 1 < n ? place(j + 1) : 0.0f;
+            sample_t[base + j] = t_cur;
+            sample_w[base + j] = atdf::sample_w(t0, t1, n, j, t_prev, t_cur, t_next);
+            t_prev = t_cur;
+            t_cur = t_next;
         }
     }
 }
@@ -610,15 +628,16 @@ int atdf_proposal_mlp_backward(const atdf_mlp_t* mlp, const atdf_segments_t* seg
 }
 
 int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, const float* logits, int32_t budget,
-                           float mass_mix, atdf_stream_t stream)
+                           float mass_mix, float mass_power, atdf_stream_t stream)
 {
-    if (!segments || !logits || num_rays < 0 || budget < 1 || !(mass_mix >= 0.0f && mass_mix <= 1.0f))
+    if (!segments || !logits || num_rays < 0 || budget < 1 || !(mass_mix >= 0.0f && mass_mix <= 1.0f) ||
+        !(mass_power >= 0.0f && mass_power <= 1.0f))
         return ATDF_ERR_INVALID_ARGUMENT;
     cudaStream_t s = (cudaStream_t)stream;
     ATDF_CUDA_TRY(cudaMemsetAsync(&segments->totals[2], 0, sizeof(int64_t), s));
     if (num_rays > 0) {
         proposal_allocate_kernel<<<(unsigned)div_up(num_rays, 128), 128, 0, s>>>(*segments, num_rays, logits, budget,
-                                                                                mass_mix);
+                                                                                mass_mix, mass_power);
         ATDF_LAUNCH_CHECK();
     }
     ATDF_CUDA_TRY(cudaMemsetAsync(&segments->ray_sample_offset[num_rays], 0, sizeof(int64_t), s));
@@ -629,15 +648,15 @@ int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, co
     return ATDF_OK;
 }
 
-int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, uint64_t seed,
-                          float* sample_t, float* sample_w, int64_t sample_capacity, int32_t* dev_error,
-                          atdf_stream_t stream)
+int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, float bin_power,
+                          uint64_t seed, float* sample_t, float* sample_w, int64_t sample_capacity,
+                          int32_t* dev_error, atdf_stream_t stream)
 {
     if (!segments || !logits || !sample_t || !sample_w || sample_capacity < 0 ||
-        !(bin_mix > 0.0f && bin_mix <= 1.0f))
+        !(bin_mix > 0.0f && bin_mix <= 1.0f) || !(bin_power >= 0.0f && bin_power <= 1.0f))
         return ATDF_ERR_INVALID_ARGUMENT;
     proposal_samples_kernel<<<seg_blocks(segments->capacity), 256, 0, (cudaStream_t)stream>>>(
-        *segments, logits, bin_mix, seed, sample_t, sample_w, sample_capacity, dev_error);
+        *segments, logits, bin_mix, bin_power, seed, sample_t, sample_w, sample_capacity, dev_error);
     ATDF_LAUNCH_CHECK();
     return ATDF_OK;
 }

@@ -162,6 +162,7 @@ class ProposalSampler {
     torch::Tensor occupancy;                  // [num_nodes, 9] float: 8 octants + whole leaf
     int64_t budget = 64;
     double mass_mix = 0.25, bin_mix = 0.2, mass_weight = 0.1;
+    double mass_power = 0.5, bin_power = 0.5;  // sample density ~ predicted density^power
     bool check_errors = false;  // read the device error words after each call (synchronises)
 
    private:

@@ -828,15 +828,15 @@ Tensor ProposalSampler::Project(HyperTreeBase& tree, GeometryTensorQO& geo, cons
                  "atdf_project_segments");
     auto logits = logits_for(tree, view, rays, nullptr);
     check_status(atdf_proposal_allocate(&view, R, logits.data_ptr<float>(), (int32_t)budget, (float)mass_mix,
-                                        stream_arg()),
+                                        (float)mass_power, stream_arg()),
                  "atdf_proposal_allocate");
-    // a ray gets at most max(budget, its segment count) samples: no host read needed
+    // a ray gets at most budget + its segment count samples: no host read needed
     const int64_t cap = R * budget + view.capacity;
     auto xt = torch::empty({std::max<int64_t>(cap, 1)}, o.options());
     auto xw = torch::empty_like(xt);
-    check_status(atdf_proposal_samples(&view, logits.data_ptr<float>(), (float)bin_mix, jitter_seed,
-                                       xt.data_ptr<float>(), xw.data_ptr<float>(), cap, err.data_ptr<int32_t>(),
-                                       stream_arg()),
+    check_status(atdf_proposal_samples(&view, logits.data_ptr<float>(), (float)bin_mix, (float)bin_power,
+                                       jitter_seed, xt.data_ptr<float>(), xw.data_ptr<float>(), cap,
+                                       err.data_ptr<int32_t>(), stream_arg()),
                  "atdf_proposal_samples");
     ProjectArgs args{&geo, &tree, 0, 0, {}, ws, xt, xw};
     auto img = project_apply(geo, args, rays);

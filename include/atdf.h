@@ -362,21 +362,27 @@ int atdf_proposal_mlp_backward(const atdf_mlp_t* mlp, const atdf_segments_t* seg
                                const float* grad_logits, const atdf_mlp_grad_t* grad_mlp, atdf_stream_t stream);
 
 /* Splits a budget of samples per ray over its segments: n = 1 +
- * floor((budget - segments of the ray) * share), share = (1 - mass_mix) *
- * predicted mass share + mass_mix * length share. Overwrites nsamp, first,
- * ray_sample_offset, totals[1] (samples) and totals[2] (max per ray). A ray
- * gets max(budget, its segment count) samples at most. */
+ * round((budget - segments of the ray) * share), share = (1 - mass_mix) *
+ * weight share + mass_mix * length share, weight = length * (predicted mean
+ * density)^mass_power (mass_power in [0, 1]: 0 is the uniform per-length
+ * rule, 1 allocates by predicted mass, 1/2 minimises the error of stratified
+ * sampling when a segment's variation scales with its density). Overwrites
+ * nsamp, first, ray_sample_offset, totals[1] (samples) and totals[2] (max
+ * per ray). A ray gets at most budget + its segment count samples. */
 int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, const float* logits, int32_t budget,
-                           float mass_mix, atdf_stream_t stream);
+                           float mass_mix, float mass_power, atdf_stream_t stream);
 
 /* Sample t and weight of every segment's nsamp samples: stratified
  * inverse-CDF draws u_j = (j + a_j) / n (a_j the interval jitter hash of
- * seed, 0.5 for seed 0) from q = (1 - bin_mix) softmax(bin logits) + bin_mix
- * / 32 over 32 equal bins; weight = 1 / (n q(t)) in units of t. Unbiased for
- * any proposal because q > 0 everywhere (bin_mix in (0, 1]). */
-int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, uint64_t seed,
-                          float* sample_t, float* sample_w, int64_t sample_capacity, int32_t* dev_error,
-                          atdf_stream_t stream);
+ * seed, 0.5 for seed 0) from q = (1 - bin_mix) softmax(bin_power * bin
+ * logits) + bin_mix / 32 over 32 equal bins (the predicted distribution
+ * raised to bin_power in [0, 1]; bin_mix in (0, 1] keeps samples
+ * everywhere). Weights are the samples' Voronoi cells within the segment,
+ * the rule of the uniform sampler (HyperTree.cu:495-512): with uniform q the
+ * result is the uniform per-node quadrature with these counts. */
+int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, float bin_power,
+                          uint64_t seed, float* sample_t, float* sample_w, int64_t sample_capacity,
+                          int32_t* dev_error, atdf_stream_t stream);
 
 /* Training loss of the proposal against seg_bins of a uniform binned forward
  * on the same segments: mean over segments of the cross-entropy of the

@@ -54,16 +54,17 @@ def features(node_min, node_max, origin, direction, seg_node, seg_ray, tmin, tma
     return f
 
 
-def allocate(ray_seg_offset, tmin, tmax, logits, budget, mass_mix):
+def allocate(ray_seg_offset, tmin, tmax, logits, budget, mass_mix, mass_power=1.0):
     """Per-segment sample counts and per-ray first indices, and the ray
-    sample offsets [R + 1]."""
+    sample offsets [R + 1]: n = 1 + round(spare * share), share mixing the
+    weight len * density^mass_power with the length."""
     R = len(ray_seg_offset) - 1
     G = int(ray_seg_offset[-1])
     n = np.zeros(G, np.int64)
     first = np.zeros(G, np.int64)
     off = np.zeros(R + 1, np.int64)
     length = (tmax - tmin).astype(np.float64)
-    mass = softplus1(logits[:G, BINS]) * length
+    mass = length * np.power(np.maximum(softplus1(logits[:G, BINS]), 1e-20), mass_power)
     for r in range(R):
         b, e = int(ray_seg_offset[r]), int(ray_seg_offset[r + 1])
         nseg = e - b
@@ -78,40 +79,46 @@ def allocate(ray_seg_offset, tmin, tmax, logits, budget, mass_mix):
             share = length[s] / lsum if lsum > 0 else 1.0 / nseg
             if msum > 0:
                 share = (1 - mass_mix) * mass[s] / msum + mass_mix * share
-            n[s] = 1 + int(np.floor(spare * share))
+            n[s] = 1 + int(np.floor(spare * share + 0.5))
             first[s] = run
             run += n[s]
         off[r + 1] = off[r] + run
     return n, first, off
 
 
-def bin_probs(lg, bin_mix):
+def bin_probs(lg, bin_mix, power=1.0):
     lg = np.asarray(lg, np.float64)
-    e = np.exp(lg - lg.max(-1, keepdims=True))
+    e = np.exp(power * (lg - lg.max(-1, keepdims=True)))
     p = e / e.sum(-1, keepdims=True)
     return p * (1 - bin_mix) + bin_mix / BINS
 
 
-def samples(tmin, tmax, nsamp, logits, bin_mix, a=None):
+def samples(tmin, tmax, nsamp, logits, bin_mix, a=None, bin_power=1.0):
     """t and weight of every segment's samples, concatenated in segment
-    order: u_j = (j + a_j) / n, inverse CDF of the binned density, weight
-    binw / (n q_b). a: per-segment arrays of jitter (None: 0.5)."""
+    order: u_j = (j + a_j) / n, inverse CDF of the binned density (the
+    predicted one raised to bin_power, mixed with uniform); weights are the
+    Voronoi cells of the placed t within the segment. a: per-segment arrays
+    of jitter (None: 0.5)."""
     ts, ws = [], []
     for s in range(len(nsamp)):
         n = int(nsamp[s])
-        p = bin_probs(logits[s, :BINS], bin_mix)
+        p = bin_probs(logits[s, :BINS], bin_mix, bin_power)
         cdf = np.concatenate([[0.0], np.cumsum(p)])
         t0, t1 = float(tmin[s]), float(tmax[s])
         binw = (t1 - t0) / BINS
+        tt = []
         for j in range(n):
             aj = 0.5 if a is None else float(a[s][j])
             u = (j + aj) / n
             b = int(np.searchsorted(cdf, u, side="right") - 1)
             b = min(max(b, 0), BINS - 1)
             frac = min(max((u - cdf[b]) / p[b], 0.0), 1.0)
-            t = min(max(t0 + (b + frac) * binw, t0), t1)
-            ts.append(t)
-            ws.append(binw / (n * p[b]))
+            tt.append(min(max(t0 + (b + frac) * binw, t0), t1))
+        for j in range(n):
+            lo = t0 if j == 0 else 0.5 * (tt[j - 1] + tt[j])
+            hi = t1 if j == n - 1 else 0.5 * (tt[j + 1] + tt[j])
+            ts.append(tt[j])
+            ws.append(hi - lo)
     return np.array(ts), np.array(ws)
 
 

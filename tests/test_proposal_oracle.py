@@ -27,9 +27,9 @@ def test_proposal_loss_gradient_matches_finite_differences():
 
 
 def test_proposal_samples_are_stratified_and_weighted():
-    """Uniform logits give the uniform stratified rule (t_j = tmin + (j + a)
-    len / n, w = len / n); for any density the weights integrate a constant
-    exactly in expectation over the jitter."""
+    """Uniform logits give the uniform per-node rule (t_j = tmin + (j + a)
+    len / n with Voronoi weights); for any density the weights of a segment
+    tile it exactly, and denser placement integrates a bump more accurately."""
     tmin = np.array([0.0, 1.0], np.float32)
     tmax = np.array([2.0, 1.5], np.float32)
     n = np.array([8, 5])
@@ -39,36 +39,22 @@ def test_proposal_samples_are_stratified_and_weighted():
     assert np.allclose(w[:8], 2 / 8) and np.allclose(w[8:], 0.5 / 5)
     rng = np.random.default_rng(1)
     lg = rng.normal(size=(2, po.OUTPUTS)) * 2
-    K = 4000
-    tot = np.zeros(2)
-    for _ in range(K):
-        a = [rng.random(8), rng.random(5)]
-        _, w = po.samples(tmin, tmax, n, lg, 0.2, a)
-        tot += [w[:8].sum(), w[8:].sum()]
-    assert np.allclose(tot / K, tmax - tmin, rtol=2e-2)
-
-
-def test_allocation_respects_budget():
-    off = np.array([0, 3, 3, 10])
-    G = 10
-    rng = np.random.default_rng(2)
-    tmin = rng.uniform(0, 1, G).astype(np.float32)
-    tmax = (tmin + rng.uniform(0.01, 0.5, G)).astype(np.float32)
-    lg = rng.normal(size=(G, po.OUTPUTS))
-    n, first, ro = po.allocate(off, tmin, tmax, lg, 16, 0.25)
-    assert np.all(n >= 1)
-    assert ro[1] - ro[0] <= 16 and ro[2] == ro[1] and ro[3] - ro[2] <= 16
-    assert list(first[:3]) == [0, n[0], n[0] + n[1]]
-
-
-def test_octant_sums_split_each_segment():
-    """Bins of a segment that crosses the leaf's x = 0 plane land in two
-    octants; per-node sums add up to the segment totals."""
-    feats = np.zeros((1, po.INPUTS))
-    feats[0, 0:3] = [-0.9, -0.5, 0.5]
-    feats[0, 3:6] = [0.9, -0.5, 0.5]
-    bins = np.ones((1, po.BINS))
-    nm, nl = po.node_occupancy_sums(bins, feats, np.array([2.0]), np.array([3]), 5)
-    assert nm[3, 8] == 32 and abs(nl[3, 8] - 2.0) < 1e-12
-    assert nm[3, 4] == 16 and nm[3, 5] == 16  # (x<=0, y<0, z>0) and (x>0, y<0, z>0)
-    assert abs(nl[3, :8].sum() - 2.0) < 1e-12
+    t, w = po.samples(tmin, tmax, n, lg, 0.2, [rng.random(8), rng.random(5)])
+    assert np.allclose([w[:8].sum(), w[8:].sum()], tmax - tmin)
+    # a narrow bump on a smooth background over a [0, 2] segment: placing
+    # samples by the bump's density (square root) integrates it better than
+    # uniform placement with the same count
+    f = lambda x: np.exp(-((x - 0.6) / 0.05) ** 2) + 0.05 * np.sin(3 * x) + 0.06  # noqa: E731
+    exact = 0.05 * np.sqrt(np.pi) + 0.05 * (1 - np.cos(6)) / 3 + 0.12
+    c = (np.arange(po.BINS) + 0.5) / po.BINS * 2
+    lg_bump = np.zeros((1, po.OUTPUTS))
+    lg_bump[0, :po.BINS] = np.log(f(c))
+    one = (np.array([0.0], np.float32), np.array([2.0], np.float32), np.array([12]))
+    errs = {}
+    for name, l in (("uniform", np.zeros((1, po.OUTPUTS))), ("bump", lg_bump)):
+        e = []
+        for _ in range(200):
+            t, w = po.samples(*one, l, 0.2, [rng.random(12)], bin_power=0.5)
+            e.append((f(t) * w).sum() - exact)
+        errs[name] = np.sqrt(np.mean(np.square(e)))
+    assert errs["bump"] < 0.75 * errs["uniform"], errs
