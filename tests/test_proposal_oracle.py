@@ -58,3 +58,30 @@ def test_proposal_samples_are_stratified_and_weighted():
             e.append((f(t) * w).sum() - exact)
         errs[name] = np.sqrt(np.mean(np.square(e)))
     assert errs["bump"] < 0.75 * errs["uniform"], errs
+
+
+def test_allocation_respects_budget():
+    off = np.array([0, 3, 3, 10])
+    G = 10
+    rng = np.random.default_rng(2)
+    tmin = rng.uniform(0, 1, G).astype(np.float32)
+    tmax = (tmin + rng.uniform(0.01, 0.5, G)).astype(np.float32)
+    lg = rng.normal(size=(G, po.OUTPUTS))
+    n, first, ro = po.allocate(off, tmin, tmax, lg, 16, 0.25, 0.5)
+    assert np.all(n >= 1)
+    seg = np.diff(off)
+    assert np.all(np.diff(ro) <= 16 + seg) and ro[2] == ro[1]
+    assert list(first[:3]) == [0, n[0], n[0] + n[1]]
+
+
+def test_octant_sums_split_each_segment():
+    """Bins of a segment that crosses the leaf's x = 0 plane land in two
+    octants; per-node sums add up to the segment totals."""
+    feats = np.zeros((1, po.INPUTS))
+    feats[0, 0:3] = [-0.9, -0.5, 0.5]
+    feats[0, 3:6] = [0.9, -0.5, 0.5]
+    bins = np.ones((1, po.BINS))
+    nm, nl = po.node_occupancy_sums(bins, feats, np.array([2.0]), np.array([3]), 5)
+    assert nm[3, 8] == 32 and abs(nl[3, 8] - 2.0) < 1e-12
+    assert nm[3, 4] == 16 and nm[3, 5] == 16  # (x<=0, y<0, z>0) and (x>0, y<0, z>0)
+    assert abs(nl[3, :8].sum() - 2.0) < 1e-12
