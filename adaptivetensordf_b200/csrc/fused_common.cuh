@@ -228,7 +228,23 @@ struct ItemInfo {
     int64_t slot;
     int nseg;
     int total;
+    double inv_total;  // 1 / total (for the sample permutation)
 };
+
+// (k * kSamplePermPrime) mod total without a 64-bit integer division: the
+// product is below 2^34 and exact in double, the quotient estimate from the
+// reciprocal is off by at most one, and q * total and the remainder are exact.
+__device__ __forceinline__ int perm_index(int k, int total, double inv_total)
+{
+    const double kp = (double)k * (double)kSamplePermPrime;
+    const double q = floor(kp * inv_total);
+    double r = kp - q * (double)total;
+    if (r < 0.0)
+        r += (double)total;
+    else if (r >= (double)total)
+        r -= (double)total;
+    return (int)r;
+}
 
 __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, float* sm, SegTab tab, uint64_t* bar,
                                               int* s_ctl, bool want_dI)
@@ -277,6 +293,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     info.slot = s_ctl[0];
     info.nseg = s_ctl[2];
     info.total = 0;
+    info.inv_total = 0.0;
     if (info.slot < 0) return info;
     const int b0 = s_ctl[1];
     if (tid < info.nseg) {
@@ -320,6 +337,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     }
     __syncthreads();
     info.total = tab.start[info.nseg];
+    info.inv_total = info.total > 0 ? 1.0 / (double)info.total : 0.0;
     return info;
 }
 
@@ -359,7 +377,7 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
                                                     int k)
 {
     SampleState s;
-    const int kk = it.total < kSamplePermPrime ? (int)(((long long)k * kSamplePermPrime) % it.total) : k;
+    const int kk = it.total < kSamplePermPrime ? perm_index(k, it.total, it.inv_total) : k;
     s.si = find_seg(tab, it.nseg, kk);
     const int j = kk - tab.start[s.si];
     const int n = tab.n[s.si];

@@ -25,7 +25,8 @@ import torch
 
 class ProposalSchedule:
     def __init__(self, tree, geo, max_samples_per_node: int, budget: int = 64, judge_every: int = 10,
-                 gate: float = 0.01, lr: float = 3e-3, warmup: int = 20, device: str = "cuda", seed: int = 1005):
+                 gate: float = 0.01, lr: float = 3e-3, warmup: int = 20, device: str = "cuda", seed: int = 1005,
+                 jitter: bool = True):
         from . import ProposalSampler
 
         self.tree, self.geo = tree, geo
@@ -42,19 +43,21 @@ class ProposalSchedule:
         self.proposal_steps = 0
         self.last_error = None
         self.last_loss = None
+        self.jitter = jitter  # False: proposal samples at stratum midpoints (seed 0)
 
     def project(self, rays, seed: int):
         """Image of this training step's rays (autograd over the field)."""
         judge = (not self.open) or (self.step % self.judge_every == 0)
         self.step += 1
+        pseed = seed if self.jitter else 0
         if not judge:
             self.proposal_steps += 1
-            return self.ps.Project(self.tree, self.geo, rays, seed)
+            return self.ps.Project(self.tree, self.geo, rays, pseed)
         self.judge_steps += 1
         img = self.ps.ProjectUniformBinned(self.tree, self.geo, rays, self.M, seed)
         if self.step > self.warmup:
             with torch.no_grad():
-                ip = self.ps.Project(self.tree, self.geo, rays, seed ^ 0x5BD1E995)
+                ip = self.ps.Project(self.tree, self.geo, rays, (seed ^ 0x5BD1E995) if self.jitter else 0)
                 ref = img.detach()
                 self.last_error = float((ip - ref).norm() / ref.norm().clamp_min(1e-30))
             self.open = self.last_error <= self.gate

@@ -155,6 +155,7 @@ class TrainOptions:
     budget: int = 64            # proposal: samples per ray
     gate: float = 0.01          # proposal: relative L2 projection error allowed vs the uniform judge
     judge_every: int = 10       # proposal: steps between judge passes while open
+    proposal_jitter: bool = True  # proposal: jittered (True) or midpoint stratum samples
     eval_every: int = 0         # steps between evaluations (0: once per epoch)
     target_psnr: float = 30.0
     time_limit: float = 0.0     # seconds of training; 0 = no limit
@@ -226,7 +227,7 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         from .proposal import ProposalSchedule
 
         prop = ProposalSchedule(tree, geo, opt.max_samples_per_node, budget=opt.budget, gate=opt.gate,
-                                judge_every=opt.judge_every, device=device)
+                                judge_every=opt.judge_every, device=device, jitter=opt.proposal_jitter)
 
     n = data.num_rays
     steps_per_epoch = n // opt.batch
@@ -310,6 +311,7 @@ def main():
     ap.add_argument("--budget", type=int, default=64)
     ap.add_argument("--gate", type=float, default=0.01)
     ap.add_argument("--judge-every", type=int, default=10)
+    ap.add_argument("--no-prop-jitter", action="store_true")
     a = ap.parse_args()
     cfg = syn.CONFIGS[a.config]
     if a.noise >= 0:
@@ -322,7 +324,8 @@ def main():
                        max_samples_per_node=a.samples or cfg.max_samples_per_node, eval_every=a.eval_every,
                        target_psnr=a.target, time_limit=a.time_limit, stop_at_target=not a.no_stop,
                        lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, loss_tv=a.tv, init_scale=a.init_scale,
-                       budget=a.budget, gate=a.gate, judge_every=a.judge_every)
+                       budget=a.budget, gate=a.gate, judge_every=a.judge_every,
+                       proposal_jitter=not a.no_prop_jitter)
     recs, reached = train(cfg, a.form, data, opt, log=lambda r: print(json.dumps(r), flush=True))
     print(json.dumps({"form": a.form, "config": a.config, "seconds_to_target": reached, "target": a.target,
                       "final_psnr": recs[-1]["psnr"] if recs else None}), flush=True)
