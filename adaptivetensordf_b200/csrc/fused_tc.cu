@@ -36,7 +36,8 @@ constexpr int kRows = 128;          // samples per tile
 constexpr int kThreadsTC = 256;     // two halves
 constexpr int kHBCols = 96;         // H0 (64) | X (16) | ones | zero pad
 constexpr int kGCols = 128;         // dA1 (64) | dA0 (64)
-constexpr int kLineWinTC = 32;      // line-gradient window entries per line
+constexpr int kLineWinTC = 32;      // line-gradient window entries per line (shared memory)
+constexpr int kLineRowsTC = 21;     // rows per line in the line-gradient MMA (3 lines <= 64 rows)
 constexpr uint32_t kTmemFwd = 256;  // columns per CTA (2 CTAs per SM)
 constexpr uint32_t kTmemBwd = 512;
 
@@ -463,11 +464,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                 item_box(p, tab.node[0], bmin, bmax);
                 const int Ln = p.field.line_len[tid];
                 int lo = 0;
-                if (Ln > kLineWinTC) {
+                if (Ln > kLineRowsTC) {
                     const float u = tid == 0 ? roi_coord(bmin[0], p.field.roi_min[0], p.field.roi_max[0])
                                              : (tid == 2 ? bmin[2] : -1.0f);
                     lo = (int)floorf(((u + 1.0f) * 0.5f) * (float)(Ln - 1)) - 2;
-                    lo = max(0, min(lo, Ln - kLineWinTC));
+                    lo = max(0, min(lo, Ln - kLineRowsTC));
                 }
                 s_lo[tid] = lo;
             }
@@ -616,17 +617,29 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
             }
             had_tile = true;
             alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
-            // scatter dX into the shared plane gradient and the line windows.
-            // Shared-memory float atomics are fast when the 32 lanes of a warp
-            // hit 32 different banks and slow when they collide: each lane walks
-            // the 16 channels starting at its own lane index, reading the values
-            // back from its row of the (now free) G buffer.
+            // scatter dX. Plane gradients: shared-memory atomics into the slot's
+            // FP32 gradient copy. Shared-memory float atomics are fast when the
+            // 32 lanes of a warp hit 32 different banks and slow when they
+            // collide: each lane walks the 16 channels from its own rotation,
+            // reading the values back from a scratch row in HB columns 48..79.
+            // Line gradients: one MMA per tile, D[row][m*16 + c] = sum over the
+            // tile's samples of tap[row][s] * (dx * plane value)[s][m*16 + c],
+            // with the tap matrix (rows m*21 + window entry) in G columns 0..63
+            // and the values in HB columns 0..47 (both operand buffers are free
+            // once the dX and dW MMAs have completed).
             {
                 float dx[16];
                 tc::ld_32x32b_x16(trow(d0, 0), dx);
                 tc::wait_ld();
+                unsigned char* hbh = sm + L.hb[h];
+                unsigned char* gh = sm + L.g[h];
+                if (real) {
+                    const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(gh + g_off(t, 8 * q)) = z4;
+                }
                 if (valid && real) {
-                    float* mine = reinterpret_cast<float*>(sm + L.g[h]) + t * (kC + 4);
+                    const int rot = lane + (lane >> 3);
 #pragma unroll 1
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], Ln = p.field.line_len[m];
@@ -636,7 +649,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                         const Corner1 l = corners1(g.lu[m], Ln);
 #pragma unroll
                         for (int q = 0; q < kC / 4; ++q)
-                            *reinterpret_cast<float4*>(mine + 4 * q) =
+                            *reinterpret_cast<float4*>(hbh + hb_off(t, 48 + 8 * q)) =
                                 make_float4(dx[4 * q] * vec[4 * q], dx[4 * q + 1] * vec[4 * q + 1],
                                             dx[4 * q + 2] * vec[4 * q + 2], dx[4 * q + 3] * vec[4 * q + 3]);
                         float* GP = gpl + p.plane_off[m];
@@ -644,35 +657,69 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                         const int t10 = (kc.y1 * Wm + kc.x0) * C, t11 = (kc.y1 * Wm + kc.x1) * C;
 #pragma unroll 4
                         for (int r = 0; r < kC; ++r) {
-                            const int c = (r + lane) & (kC - 1);
-                            const float v = mine[c];
+                            const int c = (r + rot) & (kC - 1);
+                            const float v = *reinterpret_cast<const float*>(hbh + hb_off(t, 48 + 8 * (c >> 2)) +
+                                                                            (c & 3) * 4);
                             atomicAdd(&GP[t00 + c], kc.w_nw * v);
                             atomicAdd(&GP[t01 + c], kc.w_ne * v);
                             atomicAdd(&GP[t10 + c], kc.w_sw * v);
                             atomicAdd(&GP[t11 + c], kc.w_se * v);
                         }
+                        float lv[kC];
 #pragma unroll
-                        for (int q = 0; q < kC / 4; ++q)
-                            *reinterpret_cast<float4*>(mine + 4 * q) =
-                                make_float4(dx[4 * q] * mat[4 * q], dx[4 * q + 1] * mat[4 * q + 1],
-                                            dx[4 * q + 2] * mat[4 * q + 2], dx[4 * q + 3] * mat[4 * q + 3]);
+                        for (int c = 0; c < kC; ++c) lv[c] = dx[c] * mat[c];
+                        store_bf16x8(hbh + hb_off(t, 16 * m), lv);
+                        store_bf16x8(hbh + hb_off(t, 16 * m + 8), lv + 8);
                         const int lo = s_lo[m];
                         const int i0 = l.x0 - lo, i1 = l.x1 - lo;
-                        if (i0 >= 0 && i0 < kLineWinTC && i1 >= 0 && i1 < kLineWinTC) {
-                            float* L0 = gln + (m * kLineWinTC + i0) * C;
-                            float* L1 = gln + (m * kLineWinTC + i1) * C;
-#pragma unroll 4
-                            for (int r = 0; r < kC; ++r) {
-                                const int c = (r + lane) & (kC - 1);
-                                const float v = mine[c];
-                                atomicAdd(L0 + c, l.w0 * v);
-                                atomicAdd(L1 + c, l.w1 * v);
+                        if (i0 >= 0 && i0 < kLineRowsTC && i1 >= 0 && i1 < kLineRowsTC) {
+                            if (i0 == i1) {
+                                *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i0)) =
+                                    __float2bfloat16_rn(l.w0 + l.w1);
+                            } else {
+                                *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i0)) =
+                                    __float2bfloat16_rn(l.w0);
+                                *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i1)) =
+                                    __float2bfloat16_rn(l.w1);
                             }
                         } else {  // outside the item's window: straight to global
                             for (int c = 0; c < kC; ++c) {
-                                atomicAdd(&p.gfield.line[m][l.x0 * C + c], l.w0 * mine[c]);
-                                atomicAdd(&p.gfield.line[m][l.x1 * C + c], l.w1 * mine[c]);
+                                atomicAdd(&p.gfield.line[m][l.x0 * C + c], l.w0 * lv[c]);
+                                atomicAdd(&p.gfield.line[m][l.x1 * C + c], l.w1 * lv[c]);
                             }
+                        }
+                    }
+                }
+                if (real) {
+                    tc::fence_smem_to_async();
+                    tc::fence_before_sync();
+                    half_barrier(h);
+                    if (t == 0) {
+                        tc::fence_after_sync();
+                        const uint32_t abase = tc::smem_addr(gh), bbase = tc::smem_addr(hbh);
+#pragma unroll
+                        for (int j = 0; j < kRows / 16; ++j) {
+                            const uint64_t a =
+                                tc::smem_desc(abase + j * 2 * (kGCols / 8) * 128, (kGCols / 8) * 128, 128);
+                            const uint64_t b =
+                                tc::smem_desc(bbase + j * 2 * (kHBCols / 8) * 128, (kHBCols / 8) * 128, 128);
+                            tc::mma_bf16(d1, a, b, tc::idesc_bf16(kRows, 3 * kC, 1, 1), j > 0 ? 1u : 0u);
+                        }
+                        tc::commit(&bar_mma[h]);
+                    }
+                    alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
+                    float v0[16], v1[16], v2[16];
+                    tc::ld_32x32b_x16(trow(d1, 0), v0);
+                    tc::ld_32x32b_x16(trow(d1, 16), v1);
+                    tc::ld_32x32b_x16(trow(d1, 32), v2);
+                    tc::wait_ld();
+                    if (t < 3 * kLineRowsTC) {
+                        const int m = t / kLineRowsTC, i = t % kLineRowsTC;
+                        float* dst = gln + (m * kLineWinTC + i) * C;
+#pragma unroll
+                        for (int c = 0; c < kC; ++c) {
+                            const float v = m == 0 ? v0[c] : (m == 1 ? v1[c] : v2[c]);
+                            if (v != 0.0f) atomicAdd(dst + c, v);
                         }
                     }
                 }
@@ -767,8 +814,12 @@ static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cu
     ATDF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     ATDF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, tcf::kThreadsTC, smem));
     if (per < 1) return ATDF_ERR_UNSUPPORTED;
-    // TMEM: 256 columns per forward CTA, 512 per backward CTA (512 per SM)
-    per = std::min(per, bwd ? 1 : 2);
+    // TMEM: 256 columns per forward CTA, 512 per backward CTA (512 per SM).
+    // The forward fits two CTAs per SM by shared memory and registers
+    // (launch bounds); the occupancy query reports one, so size it here.
+    int smem_sm = 0;
+    ATDF_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    per = bwd ? 1 : std::max(1, std::min(2, smem_sm / (smem + 1024)));
     fn<<<sms * per, tcf::kThreadsTC, smem, st>>>(p);
     ATDF_LAUNCH_CHECK();
     return ATDF_OK;
