@@ -11,11 +11,14 @@ drives it inside a training loop:
   kernel, Adam) and refresh the leaf occupancy, and the proposal's own
   projection of the same rays is compared with it: a relative L2 error <=
   gate (1%) opens the proposal for the following steps, above it closes it;
-* other steps, while the gate is open, train the main model through the
-  proposal's samples (a budget per ray instead of the uniform count).
+* between judge steps the main model trains through the proposal's samples
+  (a budget per ray instead of the uniform count) while the gate is open,
+  and through the plain uniform sampler while it is closed.
 
-Judge steps come every judge_every steps while the gate is open and on every
-step while it is closed. Only the gate's error is read back to the host.
+Judge steps come every judge_every_open steps while the gate is open and
+every judge_every_closed steps while it is closed (every step during the
+first `warmup` steps, to train the proposal). Only the gate's error is read
+back to the host, once per judge step after the warm-up.
 """
 
 from __future__ import annotations
@@ -26,47 +29,61 @@ import torch
 class ProposalSchedule:
     def __init__(self, tree, geo, max_samples_per_node: int, budget: int = 64, judge_every: int = 10,
                  gate: float = 0.01, lr: float = 3e-3, warmup: int = 20, device: str = "cuda", seed: int = 1005,
-                 jitter: bool = True):
-        from . import ProposalSampler
-
+                 jitter: bool = True, judge_every_closed: int = 4, sampler=None):
         self.tree, self.geo = tree, geo
         self.M = max_samples_per_node
-        self.ps = ProposalSampler(tree.NumNodes(), 64, 3, seed, device)
+        if sampler is None:
+            from . import ProposalSampler
+
+            sampler = ProposalSampler(tree.NumNodes(), 64, 3, seed, device)
+        self.ps = sampler
         self.ps.budget = budget
         self.adam = torch.optim.Adam(self.ps.parameters(), lr=lr)
         self.judge_every = judge_every
+        self.judge_every_closed = judge_every_closed
         self.gate = gate
         self.warmup = warmup
+        self.jitter = jitter  # False: proposal samples at stratum midpoints (seed 0)
         self.open = False
         self.step = 0
         self.judge_steps = 0
         self.proposal_steps = 0
+        self.uniform_steps = 0
         self.last_error = None
         self.last_loss = None
-        self.jitter = jitter  # False: proposal samples at stratum midpoints (seed 0)
+
+    def is_judge_step(self, step: int) -> bool:
+        if step < self.warmup:
+            return True
+        every = self.judge_every if self.open else self.judge_every_closed
+        return step % every == 0
 
     def project(self, rays, seed: int):
         """Image of this training step's rays (autograd over the field)."""
-        judge = (not self.open) or (self.step % self.judge_every == 0)
+        step = self.step
         self.step += 1
         pseed = seed if self.jitter else 0
-        if not judge:
-            self.proposal_steps += 1
-            return self.ps.Project(self.tree, self.geo, rays, pseed)
+        if not self.is_judge_step(step):
+            if self.open:
+                self.proposal_steps += 1
+                return self.ps.Project(self.tree, self.geo, rays, pseed)
+            self.uniform_steps += 1
+            return self.geo.ProjectRays(self.tree, rays, self.M, seed)
         self.judge_steps += 1
         img = self.ps.ProjectUniformBinned(self.tree, self.geo, rays, self.M, seed)
-        if self.step > self.warmup:
+        self.adam.zero_grad(set_to_none=True)
+        self.last_loss = self.ps.ComputeGradients(self.tree)
+        self.adam.step()
+        if step + 1 >= self.warmup:
             with torch.no_grad():
                 ip = self.ps.Project(self.tree, self.geo, rays, (seed ^ 0x5BD1E995) if self.jitter else 0)
                 ref = img.detach()
                 self.last_error = float((ip - ref).norm() / ref.norm().clamp_min(1e-30))
             self.open = self.last_error <= self.gate
-        self.adam.zero_grad(set_to_none=True)
-        self.last_loss = self.ps.ComputeGradients(self.tree)
-        self.adam.step()
         return img
 
     def stats(self):
         return {"proposal_open": self.open, "proposal_error": self.last_error,
                 "judge_steps": self.judge_steps, "proposal_steps": self.proposal_steps,
+                "uniform_steps": self.uniform_steps,
                 "proposal_loss": None if self.last_loss is None else float(self.last_loss)}

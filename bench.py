@@ -256,14 +256,18 @@ def time_to_psnr(args):
     cfg = CONFIGS["C2"]
     data = recon.make_tilt_series(cfg)
     out = {"target_db": args.psnr_target, "config": "C2 tilt series, 16384-ray batches, eval every 61 steps"}
-    for form in ("fp32", "bf16"):
+    for form in ("fp32", "bf16", "bf16+prop"):
         opt = recon.TrainOptions(epochs=args.psnr_epochs, batch=cfg.rays_per_batch,
                                  max_samples_per_node=cfg.max_samples_per_node, eval_every=61,
-                                 target_psnr=args.psnr_target, init_scale=0.05)
+                                 target_psnr=args.psnr_target, init_scale=0.05, budget=128)
         recs, reached = recon.train(cfg, form, data, opt)
         out[form] = {"seconds": reached, "best_psnr": max(r["psnr"] for r in recs), "steps": recs[-1]["step"]}
-    if out["fp32"]["seconds"] and out["bf16"]["seconds"]:
-        out["ratio_fp32_over_bf16"] = out["fp32"]["seconds"] / out["bf16"]["seconds"]
+        if form.endswith("+prop"):
+            out[form].update({k: recs[-1][k] for k in ("judge_steps", "proposal_steps", "uniform_steps",
+                                                        "proposal_error")})
+    for form in ("bf16", "bf16+prop"):
+        if out["fp32"]["seconds"] and out[form]["seconds"]:
+            out[f"ratio_fp32_over_{form}"] = out["fp32"]["seconds"] / out[form]["seconds"]
     del data
     return out
 
