@@ -66,6 +66,13 @@ class HyperTreeBase {
     torch::Tensor ComputeLocalSamples(torch::Tensor global_samples, torch::Tensor node_indices);
     std::tuple<torch::Tensor, torch::Tensor> NodeIdForPositionGPU(torch::Tensor global_samples);
     void SetErrorForActiveNodes(torch::Tensor error, const std::string& strategy);
+    // Tree structure optimisation (HyperTreeStructureOptimizer.cpp:5-392,
+    // OR-Tools MIP in the reference) solved greedily on the host: split / merge
+    // active leaves under a budget of active leaves, costs from node_error and
+    // node_max_density. Returns whether the structure changed (then the active
+    // set, prefix sums and flags are updated).
+    bool OptimizeStructure(int64_t max_active_nodes, double error_merge_factor = 1.1,
+                           double error_split_factor = 0.75);
 
     atdf_tree_t view() const;  // C view (device pointers)
 

@@ -75,6 +75,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def("ComputeLocalSamples", &HyperTreeBase::ComputeLocalSamples)
         .def("NodeIdForPositionGPU", &HyperTreeBase::NodeIdForPositionGPU)
         .def("SetErrorForActiveNodes", &HyperTreeBase::SetErrorForActiveNodes)
+        .def("OptimizeStructure", &HyperTreeBase::OptimizeStructure, py::arg("max_active_nodes"),
+             py::arg("error_merge_factor") = 1.1, py::arg("error_split_factor") = 0.75)
         .def_readonly("max_depth", &HyperTreeBase::max_depth)
         .def_readonly("use_quad_tree", &HyperTreeBase::use_quad_tree)
         .def_readwrite("node_parent", &HyperTreeBase::node_parent)

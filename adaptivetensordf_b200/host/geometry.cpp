@@ -410,7 +410,9 @@ static atdf_field_t field_view(const GeometryTensorQO& g, const std::vector<Tens
 void GeometryTensorQO::RefreshLowPrecision()
 {
     torch::NoGradGuard ng;
-    const bool fresh = planes_bf16.size() != 3;
+    bool fresh = planes_bf16.size() != 3 || lines_bf16.size() != 3;
+    for (int m = 0; m < 3 && !fresh; ++m)
+        fresh = planes_bf16[m].sizes() != planes[m].sizes() || lines_bf16[m].sizes() != lines[m].sizes();
     if (fresh) {
         planes_bf16.clear();
         lines_bf16.clear();

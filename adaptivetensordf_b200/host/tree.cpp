@@ -3,7 +3,9 @@
 // HyperTree.cu:237-259,516-610,1339-1525) over libatdf_b200.so.
 #include <ATen/cuda/CUDAContext.h>
 
+#include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "atdf_host.h"
 
@@ -386,6 +388,164 @@ void HyperTreeBase::SetErrorForActiveNodes(torch::Tensor error, const std::strin
     } else {
         TORCH_CHECK(false, "SetErrorForActiveNodes: unknown strategy ", strategy);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Tree structure optimisation. The reference solves a mixed-integer program
+// with OR-Tools / CBC (HyperTreeStructureOptimizer.cpp:5-392): every active
+// leaf chooses none / split / merge (all active siblings together), the cost
+// of a choice is error x max density with the split and merge predictions of
+// :211-323 (split: error_split_factor x own error; merge: error_merge_factor x
+// the siblings' error sum, at the siblings' max density), and the active-leaf
+// count after the change must stay within max_active_nodes (:146-206). OR-Tools
+// is not available, so the same program is solved greedily: merges with the
+// smallest cost increase per freed leaf until the budget holds, then splits
+// by gain per added leaf, paying for a split with cheaper merges while that
+// lowers the objective.
+// ---------------------------------------------------------------------------
+bool HyperTreeBase::OptimizeStructure(int64_t max_active_nodes, double error_merge_factor,
+                                      double error_split_factor)
+{
+    auto dev = node_position_min.device();
+    auto act_t = node_active.to(torch::kCPU).contiguous().clone();
+    auto cul_t = node_culled.to(torch::kCPU).contiguous();
+    auto chd_t = node_children.to(torch::kCPU).contiguous();
+    auto par_t = node_parent.to(torch::kCPU).contiguous();
+    auto err_t = node_error.to(torch::kCPU).to(torch::kFloat64).contiguous();
+    auto den_t = node_max_density.to(torch::kCPU).to(torch::kFloat64).contiguous();
+    const int64_t n = act_t.size(0);
+    const int ns = NS();
+    int32_t* act = act_t.data_ptr<int32_t>();
+    const int32_t* cul = cul_t.data_ptr<int32_t>();
+    const int32_t* chd = chd_t.data_ptr<int32_t>();
+    const int32_t* par = par_t.data_ptr<int32_t>();
+    const double* err = err_t.data_ptr<double>();
+    const double* den = den_t.data_ptr<double>();
+    auto e_of = [&](int64_t i) { return err[i] > 0 ? err[i] : 0.0; };
+    // a density never computed (negative) counts as 1
+    auto d_of = [&](int64_t i) { return den[i] >= 0 ? den[i] : 1.0; };
+
+    struct Split {
+        int64_t node;
+        double gain;
+        int cost;  // leaves added
+    };
+    struct Merge {
+        int64_t parent;
+        double loss;
+        int freed;  // leaves removed
+    };
+    std::vector<Split> splits;
+    std::vector<Merge> merges;
+    int64_t count = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (act[i] != 1) continue;
+        ++count;
+        if (chd[i * ns] >= 0) {
+            int live = 0;
+            for (int k = 0; k < ns; ++k) live += cul[chd[i * ns + k]] ? 0 : 1;
+            if (live > 0) {
+                const double none = e_of(i) * d_of(i);
+                const double split = error_split_factor * e_of(i) * d_of(i);
+                splits.push_back({i, none - split, live - 1});
+            }
+        }
+    }
+    for (int64_t p = 0; p < n; ++p) {
+        if (chd[p * ns] < 0) continue;
+        int active = 0, culled = 0;
+        double esum = 0, dmax = 0, none = 0;
+        for (int k = 0; k < ns; ++k) {
+            const int32_t c = chd[p * ns + k];
+            if (act[c] == 1) {
+                ++active;
+                esum += e_of(c);
+                dmax = std::max(dmax, d_of(c));
+                none += e_of(c) * d_of(c);
+            } else if (cul[c]) {
+                ++culled;
+            }
+        }
+        if (active == 0 || active + culled != ns) continue;
+        merges.push_back({p, error_merge_factor * esum * dmax - none, active - 1});
+    }
+    std::sort(splits.begin(), splits.end(), [](const Split& a, const Split& b) {
+        return a.gain * std::max(b.cost, 1) > b.gain * std::max(a.cost, 1);
+    });
+    std::sort(merges.begin(), merges.end(), [](const Merge& a, const Merge& b) {
+        return a.loss * std::max(b.freed, 1) < b.loss * std::max(a.freed, 1);
+    });
+    std::vector<char> split_taken(n, 0), merge_taken(n, 0), blocked(n, 0);  // blocked: parent of a split leaf
+    size_t mi = 0;
+    auto next_merge = [&]() -> int64_t {
+        while (mi < merges.size() && (blocked[merges[mi].parent] || merge_taken[merges[mi].parent])) ++mi;
+        return mi < merges.size() ? (int64_t)mi : -1;
+    };
+    // 1. meet the budget
+    while (count > max_active_nodes) {
+        const int64_t k = next_merge();
+        if (k < 0) break;
+        merge_taken[merges[k].parent] = 1;
+        count -= merges[k].freed;
+        ++mi;
+    }
+    // 2. splits, paid for by merges when the budget is full
+    for (const Split& sp : splits) {
+        if (sp.gain <= 0) break;
+        const int64_t parent = par[sp.node];
+        if (parent >= 0 && merge_taken[parent]) continue;  // its sibling group is being merged
+        if (count + sp.cost <= max_active_nodes) {
+            split_taken[sp.node] = 1;
+            if (parent >= 0) blocked[parent] = 1;
+            count += sp.cost;
+            continue;
+        }
+        // merges needed to make room, cheapest first, none involving this leaf
+        const char was_blocked = parent >= 0 ? blocked[parent] : 0;
+        if (parent >= 0) blocked[parent] = 1;
+        std::vector<int64_t> pick;
+        double loss = 0;
+        int64_t freed = 0;
+        size_t save = mi;
+        while (count + sp.cost - freed > max_active_nodes) {
+            const int64_t k = next_merge();
+            if (k < 0) break;
+            pick.push_back(k);
+            loss += merges[k].loss;
+            freed += merges[k].freed;
+            ++mi;
+        }
+        if (count + sp.cost - freed <= max_active_nodes && loss < sp.gain) {
+            for (int64_t k : pick) merge_taken[merges[k].parent] = 1;
+            split_taken[sp.node] = 1;
+            count += sp.cost - freed;
+        } else {
+            mi = save;
+            if (parent >= 0) blocked[parent] = was_blocked;
+            break;
+        }
+    }
+    bool changed = false;
+    for (int64_t i = 0; i < n; ++i) {
+        if (split_taken[i]) {
+            act[i] = 0;
+            for (int k = 0; k < ns; ++k) {
+                const int32_t c = chd[i * ns + k];
+                if (!cul[c]) act[c] = 1;
+            }
+            changed = true;
+        }
+        if (merge_taken[i]) {
+            for (int k = 0; k < ns; ++k) act[chd[i * ns + k]] = 0;
+            act[i] = 1;
+            changed = true;
+        }
+    }
+    if (changed) {
+        node_active = act_t.to(dev);
+        UpdateActive();
+    }
+    return changed;
 }
 
 }  // namespace atdf_host

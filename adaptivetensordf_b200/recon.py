@@ -140,6 +140,134 @@ def psnr(tree, geo, phantom: torch.Tensor):
 
 
 # ----------------------------------------------------------------------------
+# adaptive tree refinement
+# ----------------------------------------------------------------------------
+_PLANE_AXES = ((1, 2, 0), (0, 2, 1), (0, 1, 2))  # plane m: (u axis, v axis, third axis)
+
+
+@torch.no_grad()
+def compute_max_density(tree, geo, g: int = 12):
+    """Per active leaf, the maximum decoded density over a g^3 grid of cell
+    centres inside it (hyper_train.cpp:662-707 ComputeMaxDensity with
+    UniformGlobalSamples); written into tree.node_max_density."""
+    ids = tree.active_node_ids
+    dev = ids.device
+    c = (torch.arange(g, device=dev, dtype=torch.float32) + 0.5) / g
+    zz, yy, xx = torch.meshgrid(c, c, c, indexing="ij")
+    unit = torch.stack([xx, yy, zz], -1).reshape(-1, 3)
+    mx = torch.empty(ids.numel(), device=dev)
+    chunk = max(1, (1 << 21) // unit.shape[0])
+    for i in range(0, ids.numel(), chunk):
+        nid = ids[i:i + chunk]
+        mn = tree.node_position_min[nid]
+        sz = tree.node_position_max[nid] - mn
+        pts = (mn[:, None, :] + unit[None] * sz[:, None, :]).reshape(-1, 3).contiguous()
+        node = nid[:, None].expand(-1, unit.shape[0]).reshape(-1).contiguous()
+        dens = geo.SampleVolumeIndirect(tree, pts, node).reshape(nid.numel(), -1)
+        mx[i:i + chunk] = dens.max(1).values
+    md = tree.node_max_density.clone()
+    md[ids] = mx.to(md.device)
+    tree.node_max_density = md
+
+
+@torch.no_grad()
+def node_errors(tree, geo, data: TiltSeries, max_samples_per_node: int, rays: int = 1 << 18, batch: int = 16384,
+                seed: int = 1006):
+    """Per-node error for the structure optimisation: the FP64 per-node sums of
+    AccumulateSampleLossPerNode (geometry.cpp:33-53; hyper_train.cpp:1472-1523)
+    over a random subset of the tilt series, loss sum / weight sum, set with
+    SetErrorForActiveNodes("override")."""
+    from . import RayList
+
+    g = torch.Generator(device=data.origin.device).manual_seed(seed)
+    idx = torch.randint(0, data.num_rays, (rays,), device=data.origin.device, generator=g)
+    ls = ws = None
+    for i in range(0, rays, batch):
+        j = idx[i:i + batch]
+        _, l, w = geo.ProjectNodeError(tree, RayList(data.origin[j], data.direction[j]), max_samples_per_node, 0,
+                                       data.target[j][None])
+        ls = l if ls is None else ls + l
+        ws = w if ws is None else ws + w
+    err = torch.where(ws > 0, ls / ws.clamp_min(1e-30), torch.zeros_like(ls)).float()
+    tree.SetErrorForActiveNodes(err, "override")
+
+
+def _tree_like(tree, node_active):
+    from . import HyperTreeBase
+
+    t = HyperTreeBase(3, tree.max_depth)
+    t.settree(tree.use_quad_tree, -1.0, 1.0)
+    t.node_active = node_active.cpu().clone()
+    t.UpdateActive()
+    t.to(str(tree.node_position_min.device))
+    return t
+
+
+@torch.no_grad()
+def transfer_planes(old_tree, tree, geo, old_planes):
+    """New factor planes for the active leaves of `tree` from `old_planes` of
+    `old_tree`'s active leaves: each texel of a new leaf's plane takes the old
+    field's plane value at the texel's position (two positions along the
+    plane's third axis, averaged): a copy for unchanged leaves, the parent's
+    plane resampled for split children, the children's planes averaged and
+    placed for merged parents. Split children reproduce the parent's planes
+    exactly (the parent's bilinear cells are unions of the child's)."""
+    from . import IndirectGridSample2D
+
+    ids = tree.active_node_ids
+    dev = ids.device
+    K = ids.numel()
+    mn = tree.node_position_min[ids]
+    mxp = tree.node_position_max[ids]
+    ctr = 0.5 * (mn + mxp)
+    out = []
+    for m, P in enumerate(old_planes):
+        C, H, W = P.shape[1], P.shape[2], P.shape[3]
+        a, b, e = _PLANE_AXES[m]
+        u = torch.arange(W, device=dev, dtype=torch.float32) / (W - 1)
+        v = torch.arange(H, device=dev, dtype=torch.float32) / (H - 1)
+        vv, uu = torch.meshgrid(v, u, indexing="ij")  # [H, W]
+        vals = torch.zeros(K, H, W, C, device=dev)
+        for s in (0.25, 0.75):
+            pos = torch.empty(K, H, W, 3, device=dev)
+            pos[..., a] = mn[:, None, None, a] + uu[None] * (mxp - mn)[:, None, None, a]
+            pos[..., b] = mn[:, None, None, b] + vv[None] * (mxp - mn)[:, None, None, b]
+            pos[..., e] = (mn[:, e] + s * (mxp - mn)[:, e])[:, None, None]
+            # a hair inside the new leaf, so boundary texels find the old leaf that covers it
+            pos = ctr[:, None, None, :] + (pos - ctr[:, None, None, :]) * (1.0 - 1e-6)
+            pts = pos.reshape(-1, 3).contiguous()
+            old_id, _ = old_tree.NodeIdForPositionGPU(pts)
+            omn = old_tree.node_position_min[old_id]
+            osz = old_tree.node_position_max[old_id] - omn
+            loc = (pts - omn) / osz * 2 - 1
+            uv = torch.stack([loc[:, a], loc[:, b]], 1).contiguous()
+            slot = old_tree.node_active_prefix_sum[old_id].contiguous()
+            vals += 0.5 * IndirectGridSample2D(P.detach(), slot, uv).reshape(K, H, W, C)
+        out.append(vals.permute(0, 3, 1, 2).contiguous(memory_format=torch.channels_last))
+    return out
+
+
+def refine(tree, geo, data: TiltSeries, max_active_nodes: int, max_samples_per_node: int,
+           error_merge_factor: float = 1.1, error_split_factor: float = 0.75):
+    """One structure-refinement round (hyper_train.cpp:1886-1912): node errors,
+    max densities, the structure optimisation, and the planes moved to the new
+    leaves. Returns whether the tree changed; the caller resets the optimizer
+    (reset_optimizer_after_structure_change)."""
+    node_errors(tree, geo, data, max_samples_per_node)
+    compute_max_density(tree, geo)
+    old_tree = _tree_like(tree, tree.node_active)
+    old_planes = [p.detach() for p in geo.planes]
+    if not tree.OptimizeStructure(max_active_nodes, error_merge_factor, error_split_factor):
+        return False
+    new = transfer_planes(old_tree, tree, geo, old_planes)
+    geo.planes = [p.requires_grad_(True) for p in new]
+    geo.leaf_slot = tree.node_active_prefix_sum
+    if geo.precision == "bf16":
+        geo.RefreshLowPrecision()
+    return True
+
+
+# ----------------------------------------------------------------------------
 # training
 # ----------------------------------------------------------------------------
 @dataclass
@@ -156,6 +284,9 @@ class TrainOptions:
     gate: float = 0.01          # proposal: relative L2 projection error allowed vs the uniform judge
     judge_every: int = 10       # proposal: steps between judge passes while open
     proposal_jitter: bool = True  # proposal: jittered (True) or midpoint stratum samples
+    start_depth: int = 0        # active depth of the initial tree (0: the config's depth)
+    refine_every: int = 0       # epochs between structure refinements (0: none)
+    max_active_nodes: int = 0   # leaf budget of the refinement
     eval_every: int = 0         # steps between evaluations (0: once per epoch)
     target_psnr: float = 30.0
     time_limit: float = 0.0     # seconds of training; 0 = no limit
@@ -174,8 +305,9 @@ def plane_tv(planes):
     return tv
 
 
-def build_model(cfg, form: str, device="cuda", param_seed: int = 1003, init_scale: float = 0.5):
-    tree = syn.make_tree(cfg.tree_depth, device=device)
+def build_model(cfg, form: str, device="cuda", param_seed: int = 1003, init_scale: float = 0.5,
+                start_depth: int = 0):
+    tree = syn.make_tree(cfg.tree_depth, active_depth=start_depth or cfg.tree_depth, device=device)
     geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=param_seed, device=device,
                             init_scale=init_scale)
     geo.precision = "fp32" if form.startswith("fp32") else "bf16"
@@ -216,12 +348,15 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
     wall time (seconds, GPU-synchronised, evaluations excluded)."""
     from . import RayList
 
-    tree, geo = build_model(cfg, form, device, init_scale=opt.init_scale)
-    grid_params = list(geo.planes) + list(geo.lines)
-    dec_params = list(geo.decoder_weight) + list(geo.decoder_bias)
-    adam = torch.optim.Adam([{"params": grid_params, "lr": opt.lr_grid},
-                             {"params": dec_params, "lr": opt.lr_decoder}], fused=True)
-    sched = torch.optim.lr_scheduler.ExponentialLR(adam, opt.lr_decay)
+    tree, geo = build_model(cfg, form, device, init_scale=opt.init_scale, start_depth=opt.start_depth)
+
+    def make_optimizer(lr_grid, lr_decoder):
+        a = torch.optim.Adam([{"params": list(geo.planes) + list(geo.lines), "lr": lr_grid},
+                              {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": lr_decoder}],
+                             fused=True)
+        return a, torch.optim.lr_scheduler.ExponentialLR(a, opt.lr_decay)
+
+    adam, sched = make_optimizer(opt.lr_grid, opt.lr_decoder)
     prop = None
     if form.endswith("+prop"):
         from .proposal import ProposalSchedule
@@ -285,6 +420,15 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
                 evaluate(epoch)
                 return records, reached
         sched.step()
+        if opt.refine_every and (epoch + 1) % opt.refine_every == 0 and epoch + 1 < opt.epochs:
+            t0 = time.perf_counter()
+            if refine(tree, geo, data, opt.max_active_nodes or tree.NumActiveNodes(), opt.max_samples_per_node):
+                # reset_optimizer_after_structure_change: fresh Adam state at the current rates
+                adam, sched = make_optimizer(*[g["lr"] for g in adam.param_groups])
+            torch.cuda.synchronize()
+            t_train += time.perf_counter() - t0
+            if log:
+                log({"form": form, "refined_epoch": epoch, "leaves": int(tree.NumActiveNodes()), "t": t_train})
         if not opt.eval_every:
             evaluate(epoch)
             if reached is not None and opt.stop_at_target:
@@ -312,6 +456,9 @@ def main():
     ap.add_argument("--gate", type=float, default=0.01)
     ap.add_argument("--judge-every", type=int, default=10)
     ap.add_argument("--no-prop-jitter", action="store_true")
+    ap.add_argument("--start-depth", type=int, default=0)
+    ap.add_argument("--refine-every", type=int, default=0)
+    ap.add_argument("--max-leaves", type=int, default=0)
     a = ap.parse_args()
     cfg = syn.CONFIGS[a.config]
     if a.noise >= 0:
@@ -325,7 +472,8 @@ def main():
                        target_psnr=a.target, time_limit=a.time_limit, stop_at_target=not a.no_stop,
                        lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, loss_tv=a.tv, init_scale=a.init_scale,
                        budget=a.budget, gate=a.gate, judge_every=a.judge_every,
-                       proposal_jitter=not a.no_prop_jitter)
+                       proposal_jitter=not a.no_prop_jitter, start_depth=a.start_depth,
+                       refine_every=a.refine_every, max_active_nodes=a.max_leaves)
     recs, reached = train(cfg, a.form, data, opt, log=lambda r: print(json.dumps(r), flush=True))
     print(json.dumps({"form": a.form, "config": a.config, "seconds_to_target": reached, "target": a.target,
                       "final_psnr": recs[-1]["psnr"] if recs else None}), flush=True)
