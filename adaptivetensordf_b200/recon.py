@@ -73,6 +73,7 @@ class TiltSeries:
     clean: torch.Tensor      # [A * P] float64, device (noise-free Siddon integrals)
     volume: torch.Tensor     # [N, N, N] float32 phantom (z, y, x), device
     angles: np.ndarray
+    image_id: torch.Tensor = None  # [A * P] long: the tilt of each ray
 
     @property
     def num_rays(self):
@@ -104,7 +105,7 @@ def make_tilt_series(cfg, device="cuda", noise_seed: int = 1002) -> TiltSeries:
         if cfg.noise > 0:
             sigma = cfg.noise * float(y.max())
             y = y + torch.from_numpy(rng.normal(0.0, sigma, A * P)).to(device)
-    return TiltSeries(o_t, d_t, y.float(), clean, vol_t, angles)
+    return TiltSeries(o_t, d_t, y.float(), clean, vol_t, angles, torch.from_numpy(img).to(device))
 
 
 # ----------------------------------------------------------------------------
@@ -287,6 +288,8 @@ class TrainOptions:
     start_depth: int = 0        # active depth of the initial tree (0: the config's depth)
     refine_every: int = 0       # epochs between structure refinements (0: none)
     max_active_nodes: int = 0   # leaf budget of the refinement
+    tone_mapper: bool = False   # per-tilt multiplicative exposure (ToneMapper.cpp:161-201)
+    lr_exposure: float = 0.01   # ToneMapper.h:45 exposure_lr
     eval_every: int = 0         # steps between evaluations (0: once per epoch)
     target_psnr: float = 30.0
     time_limit: float = 0.0     # seconds of training; 0 = no limit
@@ -357,6 +360,13 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         return a, torch.optim.lr_scheduler.ExponentialLR(a, opt.lr_decay)
 
     adam, sched = make_optimizer(opt.lr_grid, opt.lr_decoder)
+    exposure = None
+    if opt.tone_mapper:
+        # PhotometricCalibration with exposure_mult: the ray integral times the
+        # tilt's exposure factor. The factors are kept at mean 1 after each
+        # step, which fixes the scale that they share with the density.
+        exposure = torch.ones(len(data.angles), device=device, requires_grad=True)
+        adam_exp = torch.optim.Adam([exposure], lr=opt.lr_exposure)
     prop = None
     if form.endswith("+prop"):
         from .proposal import ProposalSchedule
@@ -400,12 +410,21 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
                 img = prop.project(rays, seed)
             else:
                 img = geo.ProjectRays(tree, rays, opt.max_samples_per_node, seed)
-            loss = (img.view(-1) - target).pow(2).mean()
+            pred = img.view(-1)
+            if exposure is not None:
+                pred = pred * exposure[data.image_id[idx]]
+            loss = (pred - target).pow(2).mean()
             if opt.loss_tv > 0:
                 loss = loss + opt.loss_tv * plane_tv(geo.planes)
             adam.zero_grad(set_to_none=True)
+            if exposure is not None:
+                adam_exp.zero_grad(set_to_none=True)
             loss.backward()
             adam.step()
+            if exposure is not None:
+                adam_exp.step()
+                with torch.no_grad():
+                    exposure.div_(exposure.mean())
             if geo.precision == "bf16":
                 geo.RefreshLowPrecision()
             loss_acc += loss.detach().double()
@@ -459,6 +478,7 @@ def main():
     ap.add_argument("--start-depth", type=int, default=0)
     ap.add_argument("--refine-every", type=int, default=0)
     ap.add_argument("--max-leaves", type=int, default=0)
+    ap.add_argument("--tone-mapper", action="store_true")
     a = ap.parse_args()
     cfg = syn.CONFIGS[a.config]
     if a.noise >= 0:
@@ -473,7 +493,7 @@ def main():
                        lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, loss_tv=a.tv, init_scale=a.init_scale,
                        budget=a.budget, gate=a.gate, judge_every=a.judge_every,
                        proposal_jitter=not a.no_prop_jitter, start_depth=a.start_depth,
-                       refine_every=a.refine_every, max_active_nodes=a.max_leaves)
+                       refine_every=a.refine_every, max_active_nodes=a.max_leaves, tone_mapper=a.tone_mapper)
     recs, reached = train(cfg, a.form, data, opt, log=lambda r: print(json.dumps(r), flush=True))
     print(json.dumps({"form": a.form, "config": a.config, "seconds_to_target": reached, "target": a.target,
                       "final_psnr": recs[-1]["psnr"] if recs else None}), flush=True)

@@ -268,6 +268,20 @@ def time_to_psnr(args):
     for form in ("bf16", "bf16+prop"):
         if out["fp32"]["seconds"] and out[form]["seconds"]:
             out[f"ratio_fp32_over_{form}"] = out["fp32"]["seconds"] / out[form]["seconds"]
+    # the adaptive recipe of the configuration: a depth-3 start refined toward
+    # depth 4 (greedy structure optimisation, budget 1024 leaves, every 2 epochs)
+    ad = {"target_db": args.psnr_target + 0.6,
+          "recipe": "start at depth 3 (512 leaves), refine every 2 epochs, budget 1024 leaves"}
+    for form in ("fp32", "bf16"):
+        opt = recon.TrainOptions(epochs=args.psnr_epochs + 1, batch=cfg.rays_per_batch,
+                                 max_samples_per_node=cfg.max_samples_per_node, eval_every=61,
+                                 target_psnr=ad["target_db"], init_scale=0.05, start_depth=3, refine_every=2,
+                                 max_active_nodes=1024)
+        recs, reached = recon.train(cfg, form, data, opt)
+        ad[form] = {"seconds": reached, "best_psnr": max(r["psnr"] for r in recs), "steps": recs[-1]["step"]}
+    if ad["fp32"]["seconds"] and ad["bf16"]["seconds"]:
+        ad["ratio_fp32_over_bf16"] = ad["fp32"]["seconds"] / ad["bf16"]["seconds"]
+    out["adaptive_tree"] = ad
     del data
     return out
 
@@ -277,6 +291,7 @@ def run_ours(args, rank, world):
     import torch.distributed as dist
 
     import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import dp
     from adaptivetensordf_b200 import synthetic as syn
 
     local = int(os.environ.get("LOCAL_RANK", 0))
@@ -316,9 +331,7 @@ def run_ours(args, rank, world):
             img = geo.ProjectRays(tree, rays, M, 1 + k)
             loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
             img.backward(gimg)
-            if world > 1:
-                for p in params:
-                    dist.all_reduce(p.grad)
+            dp.allreduce_gradients(params, world)
             opt.step()
             opt.zero_grad(set_to_none=False)
             if bf16:

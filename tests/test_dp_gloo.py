@@ -1,0 +1,57 @@
+"""Ray data parallelism on CPU with two gloo ranks: disjoint ray shards,
+gradient averaging and node-error sums."""
+
+import os
+import socket
+
+import torch
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, out):
+    import torch.distributed as dist
+
+    from adaptivetensordf_b200 import dp
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        shards = dp.shard_permutation(1000, 64, rank, world, epoch=0)
+        p = torch.nn.Parameter(torch.zeros(5))
+        p.grad = torch.full((5,), float(rank + 1))
+        q = torch.nn.Parameter(torch.zeros(2, 2))
+        q.grad = torch.eye(2) * (rank + 1) * 10
+        dp.allreduce_gradients([p, q], world)
+        ls = torch.arange(4, dtype=torch.float64) * (rank + 1)
+        ws = torch.ones(4, dtype=torch.float64)
+        dp.allreduce_node_error(ls, ws, world)
+        out[rank] = {"shards": [s.tolist() for s in shards], "p": p.grad.tolist(), "q": q.grad.tolist(),
+                     "ls": ls.tolist(), "ws": ws.tolist()}
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_data_parallel_step():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_worker, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
+        res = dict(out)
+    a, b = res[0], res[1]
+    assert len(a["shards"]) == len(b["shards"]) == 1000 // (2 * 64)
+    for sa, sb in zip(a["shards"], b["shards"]):
+        assert len(sa) == len(sb) == 64 and not set(sa) & set(sb)
+    for r in (a, b):
+        assert r["p"] == [1.5] * 5
+        assert r["q"] == [[15.0, 0.0], [0.0, 15.0]]
+        assert r["ls"] == [0.0, 3.0, 6.0, 9.0] and r["ws"] == [2.0] * 4
