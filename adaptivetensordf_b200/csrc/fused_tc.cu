@@ -4,9 +4,11 @@
 // decoder 16 -> 64 -> 64 -> 1 (the reference's FCBlock default with one
 // hidden layer of 64; hyperacorn/csrc/geometry/Modules.h:68-109).
 //
-// A CTA has two halves of 128 threads; each half owns a 128-sample tile, one
-// thread per sample (= one TMEM lane / accumulator row). Both halves share
-// the work item's planes (staged by TMA) and, in the backward, its shared
+// A forward CTA has two halves of 128 threads; each half owns a 128-sample
+// tile, one thread per sample (= one TMEM lane / accumulator row). A backward
+// CTA has two halves of 256 threads, two per sample row, each of the pair
+// taking half the channels and half the hidden columns. Both halves share the
+// work item's planes (staged by TMA) and, in the backward, its shared
 // plane-gradient copy. Per tile:
 //   forward  X[128x16] -> D0 = X W0^T -> H0 = silu(D0 + b0)
 //            D1 = H0 W1^T -> silu(D1 + b1) . w2 + b2 -> softplus -> rho * w
@@ -193,50 +195,19 @@ __device__ __forceinline__ void gather_features(const FusedParams& p, const unsi
 }
 
 
-// Bilinear plane value and linear line value of plane / line m for the 16
-// channels of one sample (the backward's recomputation of its gathers).
-__device__ __forceinline__ void gather_plane(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
-                                             float (&mat)[kC], float (&vec)[kC])
-{
-    const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
-    const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
-    const Corner1 l = corners1(g.lu[m], L);
-    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
-    const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        float a[8], b[8], c[8], d[8], v0[8], v1[8];
-        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x0) * kC + 8 * half) * 2), a);
-        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x1) * kC + 8 * half) * 2), b);
-        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x0) * kC + 8 * half) * 2), c);
-        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x1) * kC + 8 * half) * 2), d);
-        unpack_bf16x8(__ldg(V + l.x0 * 2 + half), v0);
-        unpack_bf16x8(__ldg(V + l.x1 * 2 + half), v1);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            float acc = a[i] * k.w_nw;
-            acc = fmaf(b[i], k.w_ne, acc);
-            acc = fmaf(c[i], k.w_sw, acc);
-            acc = fmaf(d[i], k.w_se, acc);
-            mat[8 * half + i] = acc;
-            vec[8 * half + i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
-        }
-    }
-}
-
 __device__ __forceinline__ void load_weights_tc(const FusedParams& p, unsigned char* sm, const TCSmem& L)
 {
     const atdf_mlp_t& m = p.mlp;
-    for (int i = threadIdx.x; i < kH * kC; i += kThreadsTC) {
+    for (int i = threadIdx.x; i < kH * kC; i += blockDim.x) {
         const int n = i / kC, f = i % kC;
         *reinterpret_cast<__nv_bfloat16*>(sm + L.w0 + w0_off(n, f)) = __float2bfloat16_rn(m.weight[0][i]);
     }
-    for (int i = threadIdx.x; i < kH * kH; i += kThreadsTC) {
+    for (int i = threadIdx.x; i < kH * kH; i += blockDim.x) {
         const int n = i / kH, k = i % kH;
         *reinterpret_cast<__nv_bfloat16*>(sm + L.w1 + w1_off(n, k)) = __float2bfloat16_rn(m.weight[1][i]);
     }
     float* bias = reinterpret_cast<float*>(sm + L.bias);
-    for (int i = threadIdx.x; i < kH; i += kThreadsTC) {
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
         bias[i] = m.bias[0][i];
         bias[kH + i] = m.bias[1][i];
         bias[2 * kH + i] = m.weight[2][i];
@@ -409,7 +380,88 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
     if (tid < 32) tc::tmem_dealloc(s_tmem, kTmemFwd);
 }
 
-__global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams p)
+// ---------------------------------------------------------------------------
+// Backward with two threads per sample row: 512 threads = two halves x two
+// channel groups of 128 threads. Group g of a half owns channels 8g..8g+7 of
+// the features and columns 32g..32g+31 of every 64-wide layer, so each
+// thread carries half the registers of the 256-thread kernel and an SM runs
+// 16 warps instead of 8 within the same shared memory and TMEM (a 256-thread
+// version with one thread per row ran 4.9 ms where this one runs 4.0 ms on
+// 16384 rays of the depth-4 workload).
+// ---------------------------------------------------------------------------
+constexpr int kThreadsB2 = 512;
+
+__device__ __forceinline__ void half_barrier2(int h) { asm volatile("bar.sync %0, 256;" ::"r"(1 + h) : "memory"); }
+
+// Bilinear plane values and linear line values of plane / line m for the 8
+// channels cb..cb+7 of one sample.
+__device__ __forceinline__ void gather_half(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
+                                            int cb, float (&mat)[8], float (&vec)[8])
+{
+    const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
+    const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
+    const Corner1 l = corners1(g.lu[m], L);
+    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
+    const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
+    float a[8], b[8], c[8], d[8], v0[8], v1[8];
+    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x0) * kC + cb) * 2), a);
+    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x1) * kC + cb) * 2), b);
+    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x0) * kC + cb) * 2), c);
+    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x1) * kC + cb) * 2), d);
+    unpack_bf16x8(__ldg(V + l.x0 * 2 + (cb >> 3)), v0);
+    unpack_bf16x8(__ldg(V + l.x1 * 2 + (cb >> 3)), v1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float acc = a[i] * k.w_nw;
+        acc = fmaf(b[i], k.w_ne, acc);
+        acc = fmaf(c[i], k.w_sw, acc);
+        acc = fmaf(d[i], k.w_se, acc);
+        mat[i] = acc;
+        vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
+    }
+}
+
+// Features (channels cb..cb+7) of tile row t into HB; returns validity.
+__device__ __forceinline__ bool tile_features_half(const FusedParams& p, unsigned char* sm, const TCSmem& L,
+                                                   const SegTab& tab, const ItemInfo& it, bool real, int h, int k,
+                                                   int t, int cb, float& w, int& si, SampleGeo& g)
+{
+    const bool valid = k < it.total;
+    float f[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = 0.0f;
+    w = 0.0f;
+    si = -1;
+    if (valid) {
+        const SampleState st = sample_state(p, tab, it, k);
+        w = st.w;
+        si = st.si;
+        if (real) {
+            g = sample_geo_fast(p, tab, st.si, st.pos);
+            // planes 2, 1, 0: the same operation order as gather_features
+#pragma unroll
+            for (int m = 2; m >= 0; --m) {
+                float mat[8], vec[8];
+                gather_half(p, sm, g, m, cb, mat, vec);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) f[i] = m == 2 ? mat[i] * vec[i] : fmaf(mat[i], vec[i], f[i]);
+            }
+        }
+    }
+    store_bf16x8(sm + L.hb[h] + hb_off(t, kH + cb), f);
+    return valid;
+}
+
+// Scratch float j (0..47) of sample t: HB columns 48..79 for j < 16, G
+// columns 64..127 (free once the dX and dW MMAs have read them) for the rest.
+__device__ __forceinline__ float* scratch2(unsigned char* hbh, unsigned char* gh, int t, int j)
+{
+    if (j < 16) return reinterpret_cast<float*>(hbh + hb_off(t, 48 + 8 * (j >> 2)) + (j & 3) * 4);
+    const int q = j - 16;
+    return reinterpret_cast<float*>(gh + g_off(t, 64 + 8 * (q >> 2)) + (q & 3) * 4);
+}
+
+__global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams p)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar_tma;
@@ -417,8 +469,12 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
     __shared__ uint32_t s_tmem;
     __shared__ int s_ctl[4];
     __shared__ int s_lo[3];
+    __shared__ float s_z[2][2][kRows];  // partial last-layer sums [half][group][row]
     const TCSmem L(p.plane_off[3], true);
-    const int tid = threadIdx.x, h = tid / kRows, t = tid % kRows, lane = tid & 31;
+    const int tid = threadIdx.x, h = tid >> 8, grp = (tid >> 7) & 1, t = tid & (kRows - 1), lane = tid & 31;
+    const int cb = 8 * grp;       // channels of this group
+    const int col0 = 32 * grp;    // hidden columns of this group
+    const bool issuer = (tid & 255) == 0;
     if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemBwd);
     if (tid == 0) {
         mbar_init(&bar_tma, 1);
@@ -427,7 +483,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
     }
     load_weights_tc(p, sm, L);
     // ones column (80) and zero padding (81..95) of both HB buffers
-    for (int i = tid; i < 2 * kRows; i += kThreadsTC) {
+    for (int i = tid; i < 2 * kRows; i += kThreadsB2) {
         const int hh = i / kRows, s = i % kRows;
         float v[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         store_bf16x8(sm + L.hb[hh] + hb_off(s, 80), v);
@@ -448,17 +504,20 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
     const int plane_elems = p.plane_off[3];
     float* gpl = reinterpret_cast<float*>(sm + L.gplanes);
     float* gln = reinterpret_cast<float*>(sm + L.gline);
+    unsigned char* hbh = sm + L.hb[h];
+    unsigned char* gh = sm + L.g[h];
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true, had_tile = false;
-    float gw2a = 0.f, gw2b = 0.f, gb2 = 0.f;  // lane owns last-layer columns 2*lane, 2*lane+1
+    float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group
+    const int rot = lane + (lane >> 3);
     while (alive) {
         const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real) {
-            for (int i = tid * 4; i < plane_elems; i += kThreadsTC * 4)
+            for (int i = tid * 4; i < plane_elems; i += kThreadsB2 * 4)
                 *reinterpret_cast<float4*>(gpl + i) = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsTC) gln[i] = 0.0f;
+            for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsB2) gln[i] = 0.0f;
             if (tid < 3) {
                 float bmin[3], bmax[3];
                 item_box(p, tab.node[0], bmin, bmax);
@@ -481,75 +540,87 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
         }
         alive = __syncthreads_and(alive);
         for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
-            bool valid = false;
             SampleGeo g;
-            float w, ts;
+            float w;
             int si;
-            valid = tile_features(p, sm, L, tab, it, real, h, t0 + t, t, w, si, g, ts);
+            const bool valid = tile_features_half(p, sm, L, tab, it, real, h, t0 + t, t, cb, w, si, g);
             const float dIw = valid ? tab.acc[si] * w : 0.0f;
             tc::fence_smem_to_async();
             tc::fence_before_sync();
-            half_barrier(h);
-            if (t == 0) {
+            half_barrier2(h);
+            if (issuer) {
                 tc::fence_after_sync();
                 issue_l0(sm, L, h, d0);
                 tc::commit(&bar_mma[h]);
             }
             alive = wait_mma(&bar_mma[h], mma_phase, p.err);
-            epilogue_l0(sm, L, h, t, d0);
+            // H0 = silu(D0 + b0), this group's 32 columns
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                float v[16], bb[16];
+                tc::ld_32x32b_x16(trow(d0, col0 + 16 * j), v);
+                ld16(bias + col0 + 16 * j, bb);
+                tc::wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + bb[i]);
+                store_bf16x8(hbh + hb_off(t, col0 + 16 * j), v);
+                store_bf16x8(hbh + hb_off(t, col0 + 16 * j + 8), v + 8);
+            }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
-            half_barrier(h);
-            if (t == 0) {
+            half_barrier2(h);
+            if (issuer) {
                 tc::fence_after_sync();
                 issue_l1(sm, L, h, d1);
                 tc::commit(&bar_mma[h]);
             }
             alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
-            // last layer: z, dz; dA1 = dz w2 silu'(A1) into G columns 0..63
-            float a1[kH];
+            // last layer: partial z over this group's columns
+            float a1[32];
 #pragma unroll
-            for (int j = 0; j < kH / 16; ++j) {
+            for (int j = 0; j < 2; ++j) {
                 float v[16], bb[16];
-                tc::ld_32x32b_x16(trow(d1, 16 * j), v);
-                ld16(bias + kH + 16 * j, bb);
+                tc::ld_32x32b_x16(trow(d1, col0 + 16 * j), v);
+                ld16(bias + kH + col0 + 16 * j, bb);
                 tc::wait_ld();
 #pragma unroll
                 for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bb[i];
             }
-            float z = bias[3 * kH];
+            float zp = 0.f;
 #pragma unroll
-            for (int j = 0; j < kH / 16; ++j) {
+            for (int j = 0; j < 2; ++j) {
                 float ww[16];
-                ld16(bias + 2 * kH + 16 * j, ww);
+                ld16(bias + 2 * kH + col0 + 16 * j, ww);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) z = fmaf(silu(a1[16 * j + i]), ww[i], z);
+                for (int i = 0; i < 16; ++i) zp = fmaf(silu(a1[16 * j + i]), ww[i], zp);
             }
+            s_z[h][grp][t] = zp;
+            half_barrier2(h);
+            const float z = s_z[h][0][t] + s_z[h][1][t] + bias[3 * kH];
             const float dz = dIw * act_grad(lact, z, beta);
-            {
-                float da[16];
+            // dA1 = dz w2 silu'(A1) into G columns col0..col0+31
 #pragma unroll
-                for (int j = 0; j < kH / 16; ++j) {
-                    float ww[16];
-                    ld16(bias + 2 * kH + 16 * j, ww);
+            for (int j = 0; j < 2; ++j) {
+                float ww[16], da[16];
+                ld16(bias + 2 * kH + col0 + 16 * j, ww);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) da[i] = dz * ww[i] * silu_grad(a1[16 * j + i]);
-                    store_bf16x8(sm + L.g[h] + g_off(t, 16 * j), da);
-                    store_bf16x8(sm + L.g[h] + g_off(t, 16 * j + 8), da + 8);
-                }
+                for (int i = 0; i < 16; ++i) da[i] = dz * ww[i] * silu_grad(a1[16 * j + i]);
+                store_bf16x8(gh + g_off(t, col0 + 16 * j), da);
+                store_bf16x8(gh + g_off(t, col0 + 16 * j + 8), da + 8);
             }
-            // last-layer weight gradient: reduce dz * silu(a1[k]) over the warp's
-            // 32 rows, halving the value set each round; lane ends with 2 columns
+            // last-layer weight gradient: reduce dz * silu(a1[k]) over the
+            // warp's 32 rows, halving the value set each round; the lane ends
+            // with one column
             {
 #pragma unroll
-                for (int k = 0; k < kH; ++k) a1[k] = dz * silu(a1[k]);
-                int n = kH;
+                for (int k = 0; k < 32; ++k) a1[k] = dz * silu(a1[k]);
+                int n = 32;
 #pragma unroll
                 for (int off = 16; off >= 1; off >>= 1) {
                     const bool upper = (lane & off) != 0;
                     n >>= 1;
 #pragma unroll
-                    for (int k = 0; k < kH / 2; ++k) {
+                    for (int k = 0; k < 16; ++k) {
                         if (k < n) {
                             const float send = upper ? a1[k] : a1[k + n];
                             const float keep = upper ? a1[k + n] : a1[k];
@@ -557,19 +628,20 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                         }
                     }
                 }
-                gw2a += a1[0];
-                gw2b += a1[1];
-                float s = dz;
+                gw2 += a1[0];
+                if (grp == 0) {
+                    float s = dz;
 #pragma unroll
-                for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-                if (lane == 0) gb2 += s;
+                    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+                    if (lane == 0) gb2 += s;
+                }
             }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
-            half_barrier(h);
-            if (t == 0) {  // dH0 = dA1 W1 into the D1 columns
+            half_barrier2(h);
+            if (issuer) {  // dH0 = dA1 W1 into the D1 columns
                 tc::fence_after_sync();
-                const uint32_t abase = tc::smem_addr(sm + L.g[h]), bbase = tc::smem_addr(sm + L.w1);
+                const uint32_t abase = tc::smem_addr(gh), bbase = tc::smem_addr(sm + L.w1);
 #pragma unroll
                 for (int j = 0; j < kH / 16; ++j) {
                     const uint64_t a = tc::smem_desc(abase + j * 256, 128, (kGCols / 8) * 128);
@@ -579,26 +651,26 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                 tc::commit(&bar_mma[h]);
             }
             alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
-            // dA0 = dH0 silu'(A0) into G columns 64..127 (A0 = D0 + b0)
+            // dA0 = dH0 silu'(A0) into G columns 64 + col0.. (A0 = D0 + b0)
 #pragma unroll
-            for (int j = 0; j < kH / 16; ++j) {
+            for (int j = 0; j < 2; ++j) {
                 float gv[16], av[16], da[16], bb[16];
-                tc::ld_32x32b_x16(trow(d1, 16 * j), gv);
-                tc::ld_32x32b_x16(trow(d0, 16 * j), av);
-                ld16(bias + 16 * j, bb);
+                tc::ld_32x32b_x16(trow(d1, col0 + 16 * j), gv);
+                tc::ld_32x32b_x16(trow(d0, col0 + 16 * j), av);
+                ld16(bias + col0 + 16 * j, bb);
                 tc::wait_ld();
 #pragma unroll
                 for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bb[i]);
-                store_bf16x8(sm + L.g[h] + g_off(t, kH + 16 * j), da);
-                store_bf16x8(sm + L.g[h] + g_off(t, kH + 16 * j + 8), da + 8);
+                store_bf16x8(gh + g_off(t, kH + col0 + 16 * j), da);
+                store_bf16x8(gh + g_off(t, kH + col0 + 16 * j + 8), da + 8);
             }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
-            half_barrier(h);
-            if (t == 0) {
+            half_barrier2(h);
+            if (issuer) {
                 tc::fence_after_sync();
                 // dX = dA0 W0 into the D0 columns 0..15
-                const uint32_t abase = tc::smem_addr(sm + L.g[h] + (kH / 8) * 128), bbase = tc::smem_addr(sm + L.w0);
+                const uint32_t abase = tc::smem_addr(gh + (kH / 8) * 128), bbase = tc::smem_addr(sm + L.w0);
 #pragma unroll
                 for (int j = 0; j < kH / 16; ++j) {
                     const uint64_t a = tc::smem_desc(abase + j * 256, 128, (kGCols / 8) * 128);
@@ -606,7 +678,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                     tc::mma_bf16(d0, a, b, tc::idesc_bf16(kRows, kC, 0, 1), j > 0);
                 }
                 // [dW1 db1; dW0 db0] += [dA1 | dA0]^T [H0 | X | 1]
-                const uint32_t gbase = tc::smem_addr(sm + L.g[h]), hbase = tc::smem_addr(sm + L.hb[h]);
+                const uint32_t gbase = tc::smem_addr(gh), hbase = tc::smem_addr(hbh);
 #pragma unroll
                 for (int j = 0; j < kRows / 16; ++j) {
                     const uint64_t a = tc::smem_desc(gbase + j * 2 * (kGCols / 8) * 128, (kGCols / 8) * 128, 128);
@@ -617,115 +689,110 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
             }
             had_tile = true;
             alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
-            // scatter dX. Plane gradients: shared-memory atomics into the slot's
-            // FP32 gradient copy. Shared-memory float atomics are fast when the
-            // 32 lanes of a warp hit 32 different banks and slow when they
-            // collide: each lane walks the 16 channels from its own rotation,
-            // reading the values back from a scratch row in HB columns 48..79.
-            // Line gradients: one MMA per tile, D[row][m*16 + c] = sum over the
-            // tile's samples of tap[row][s] * (dx * plane value)[s][m*16 + c],
-            // with the tap matrix (rows m*21 + window entry) in G columns 0..63
-            // and the values in HB columns 0..47 (both operand buffers are free
-            // once the dX and dW MMAs have completed).
-            {
-                float dx[16];
-                tc::ld_32x32b_x16(trow(d0, 0), dx);
-                tc::wait_ld();
-                unsigned char* hbh = sm + L.hb[h];
-                unsigned char* gh = sm + L.g[h];
-                if (real) {
+            // scatter, phase 1 (own channels): dX * line values into the
+            // scratch row, dX * plane values as the line MMA's B operand, and
+            // (group 0) the tap column of the line MMA's A operand
+            float dx[8];
+            tc::ld_32x32b_x8(trow(d0, cb), dx);
+            tc::wait_ld();
+            if (real) {
+                if (grp == 0) {
                     const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
                     for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(gh + g_off(t, 8 * q)) = z4;
                 }
-                if (valid && real) {
-                    const int rot = lane + (lane >> 3);
+                if (valid) {
 #pragma unroll 1
                     for (int m = 0; m < 3; ++m) {
-                        const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], Ln = p.field.line_len[m];
-                        float mat[kC], vec[kC];
-                        gather_plane(p, sm, g, m, mat, vec);
-                        const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
-                        const Corner1 l = corners1(g.lu[m], Ln);
+                        const int Ln = p.field.line_len[m];
+                        float mat[8], vec[8], lv[8];
+                        gather_half(p, sm, g, m, cb, mat, vec);
 #pragma unroll
-                        for (int q = 0; q < kC / 4; ++q)
-                            *reinterpret_cast<float4*>(hbh + hb_off(t, 48 + 8 * q)) =
+                        for (int q = 0; q < 2; ++q)
+                            *reinterpret_cast<float4*>(scratch2(hbh, gh, t, 16 * m + cb + 4 * q)) =
                                 make_float4(dx[4 * q] * vec[4 * q], dx[4 * q + 1] * vec[4 * q + 1],
                                             dx[4 * q + 2] * vec[4 * q + 2], dx[4 * q + 3] * vec[4 * q + 3]);
-                        float* GP = gpl + p.plane_off[m];
-                        const int t00 = (kc.y0 * Wm + kc.x0) * C, t01 = (kc.y0 * Wm + kc.x1) * C;
-                        const int t10 = (kc.y1 * Wm + kc.x0) * C, t11 = (kc.y1 * Wm + kc.x1) * C;
-#pragma unroll 4
-                        for (int r = 0; r < kC; ++r) {
-                            const int c = (r + rot) & (kC - 1);
-                            const float v = *reinterpret_cast<const float*>(hbh + hb_off(t, 48 + 8 * (c >> 2)) +
-                                                                            (c & 3) * 4);
-                            atomicAdd(&GP[t00 + c], kc.w_nw * v);
-                            atomicAdd(&GP[t01 + c], kc.w_ne * v);
-                            atomicAdd(&GP[t10 + c], kc.w_sw * v);
-                            atomicAdd(&GP[t11 + c], kc.w_se * v);
-                        }
-                        float lv[kC];
 #pragma unroll
-                        for (int c = 0; c < kC; ++c) lv[c] = dx[c] * mat[c];
-                        store_bf16x8(hbh + hb_off(t, 16 * m), lv);
-                        store_bf16x8(hbh + hb_off(t, 16 * m + 8), lv + 8);
+                        for (int c = 0; c < 8; ++c) lv[c] = dx[c] * mat[c];
+                        store_bf16x8(hbh + hb_off(t, 16 * m + cb), lv);
+                        const Corner1 l = corners1(g.lu[m], Ln);
                         const int lo = s_lo[m];
                         const int i0 = l.x0 - lo, i1 = l.x1 - lo;
                         if (i0 >= 0 && i0 < kLineRowsTC && i1 >= 0 && i1 < kLineRowsTC) {
-                            if (i0 == i1) {
-                                *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i0)) =
-                                    __float2bfloat16_rn(l.w0 + l.w1);
-                            } else {
-                                *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i0)) =
-                                    __float2bfloat16_rn(l.w0);
-                                *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i1)) =
-                                    __float2bfloat16_rn(l.w1);
+                            if (grp == 0) {
+                                if (i0 == i1) {
+                                    *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i0)) =
+                                        __float2bfloat16_rn(l.w0 + l.w1);
+                                } else {
+                                    *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i0)) =
+                                        __float2bfloat16_rn(l.w0);
+                                    *reinterpret_cast<__nv_bfloat16*>(gh + g_off(t, m * kLineRowsTC + i1)) =
+                                        __float2bfloat16_rn(l.w1);
+                                }
                             }
                         } else {  // outside the item's window: straight to global
-                            for (int c = 0; c < kC; ++c) {
-                                atomicAdd(&p.gfield.line[m][l.x0 * C + c], l.w0 * lv[c]);
-                                atomicAdd(&p.gfield.line[m][l.x1 * C + c], l.w1 * lv[c]);
+                            for (int c = 0; c < 8; ++c) {
+                                atomicAdd(&p.gfield.line[m][l.x0 * C + cb + c], l.w0 * lv[c]);
+                                atomicAdd(&p.gfield.line[m][l.x1 * C + cb + c], l.w1 * lv[c]);
                             }
                         }
                     }
                 }
-                if (real) {
-                    tc::fence_smem_to_async();
-                    tc::fence_before_sync();
-                    half_barrier(h);
-                    if (t == 0) {
-                        tc::fence_after_sync();
-                        const uint32_t abase = tc::smem_addr(gh), bbase = tc::smem_addr(hbh);
+                tc::fence_smem_to_async();
+                tc::fence_before_sync();
+                half_barrier2(h);
+                if (issuer) {  // line gradients of the tile (overlaps the plane atomics)
+                    tc::fence_after_sync();
+                    const uint32_t abase = tc::smem_addr(gh), bbase = tc::smem_addr(hbh);
 #pragma unroll
-                        for (int j = 0; j < kRows / 16; ++j) {
-                            const uint64_t a =
-                                tc::smem_desc(abase + j * 2 * (kGCols / 8) * 128, (kGCols / 8) * 128, 128);
-                            const uint64_t b =
-                                tc::smem_desc(bbase + j * 2 * (kHBCols / 8) * 128, (kHBCols / 8) * 128, 128);
-                            tc::mma_bf16(d1, a, b, tc::idesc_bf16(kRows, 3 * kC, 1, 1), j > 0 ? 1u : 0u);
-                        }
-                        tc::commit(&bar_mma[h]);
+                    for (int j = 0; j < kRows / 16; ++j) {
+                        const uint64_t a =
+                            tc::smem_desc(abase + j * 2 * (kGCols / 8) * 128, (kGCols / 8) * 128, 128);
+                        const uint64_t b =
+                            tc::smem_desc(bbase + j * 2 * (kHBCols / 8) * 128, (kHBCols / 8) * 128, 128);
+                        tc::mma_bf16(d1, a, b, tc::idesc_bf16(kRows, 3 * kC, 1, 1), j > 0 ? 1u : 0u);
                     }
-                    alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
-                    float v0[16], v1[16], v2[16];
-                    tc::ld_32x32b_x16(trow(d1, 0), v0);
-                    tc::ld_32x32b_x16(trow(d1, 16), v1);
-                    tc::ld_32x32b_x16(trow(d1, 32), v2);
-                    tc::wait_ld();
-                    if (t < 3 * kLineRowsTC) {
-                        const int m = t / kLineRowsTC, i = t % kLineRowsTC;
-                        float* dst = gln + (m * kLineWinTC + i) * C;
-#pragma unroll
-                        for (int c = 0; c < kC; ++c) {
-                            const float v = m == 0 ? v0[c] : (m == 1 ? v1[c] : v2[c]);
-                            if (v != 0.0f) atomicAdd(dst + c, v);
+                    tc::commit(&bar_mma[h]);
+                }
+                // scatter, phase 2: plane gradients, 16 channels in lane-rotated
+                // order (different banks per lane); group 0 adds the two upper
+                // corners, group 1 the two lower ones
+                if (valid) {
+#pragma unroll 1
+                    for (int m = 0; m < 3; ++m) {
+                        const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
+                        const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
+                        float* GP = gpl + p.plane_off[m];
+                        const int ya = grp == 0 ? kc.y0 : kc.y1;
+                        const float wa = grp == 0 ? kc.w_nw : kc.w_sw, wb = grp == 0 ? kc.w_ne : kc.w_se;
+                        const int ta = (ya * Wm + kc.x0) * C, tb = (ya * Wm + kc.x1) * C;
+#pragma unroll 4
+                        for (int r = 0; r < kC; ++r) {
+                            const int c = (r + rot) & (kC - 1);
+                            const float v = *scratch2(hbh, gh, t, 16 * m + c);
+                            atomicAdd(&GP[ta + c], wa * v);
+                            atomicAdd(&GP[tb + c], wb * v);
                         }
+                    }
+                }
+                alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
+                float v0[8], v1[8], v2[8];
+                tc::ld_32x32b_x8(trow(d1, cb), v0);
+                tc::ld_32x32b_x8(trow(d1, kC + cb), v1);
+                tc::ld_32x32b_x8(trow(d1, 2 * kC + cb), v2);
+                tc::wait_ld();
+                if (t < 3 * kLineRowsTC) {
+                    const int m = t / kLineRowsTC, i = t % kLineRowsTC;
+                    float* dst = gln + (m * kLineWinTC + i) * C + cb;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const float v = m == 0 ? v0[c] : (m == 1 ? v1[c] : v2[c]);
+                        if (v != 0.0f) atomicAdd(dst + c, v);
                     }
                 }
             }
             tc::fence_before_sync();
-            half_barrier(h);
+            half_barrier2(h);
         }
         alive = __syncthreads_and(alive);
         if (real) {
@@ -733,11 +800,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
                 const float* src = gpl + p.plane_off[m];
-                for (int i = tid * 4; i < pf; i += kThreadsTC * 4)
+                for (int i = tid * 4; i < pf; i += kThreadsB2 * 4)
                     atomicAdd(reinterpret_cast<float4*>(dst + i), *reinterpret_cast<const float4*>(src + i));
                 const int Ln = p.field.line_len[m];
                 const int lo = s_lo[m];
-                for (int i = tid; i < kLineWinTC * C; i += kThreadsTC) {
+                for (int i = tid; i < kLineWinTC * C; i += kThreadsB2) {
                     const int e = lo + i / C;
                     const float v = gln[m * kLineWinTC * C + i];
                     if (e < Ln && v != 0.0f) atomicAdd(&p.gfield.line[m][e * C + (i % C)], v);
@@ -746,11 +813,13 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
         }
         __syncthreads();
     }
-    // decoder gradients: the TMEM accumulator rows of this half
+    // decoder gradients: the TMEM accumulator rows of this half (group 0 reads
+    // columns 0..47, group 1 columns 48..95)
     if (had_tile) {
         tc::fence_after_sync();
 #pragma unroll
-        for (int j = 0; j < kHBCols / 16; ++j) {
+        for (int jj = 0; jj < 3; ++jj) {
+            const int j = 3 * grp + jj;
             float v[16];
             tc::ld_32x32b_x16(trow(dacc, 16 * j), v);
             tc::wait_ld();
@@ -768,14 +837,13 @@ __global__ void __launch_bounds__(kThreadsTC, 1) tc_backward_kernel(FusedParams 
             }
         }
     }
-    // last layer: lane l's two columns are given by the halving order above
+    // last layer: lane l's column within its group's 32, by the halving order above
     {
         int colbits = 0;
         for (int off = 16, b = 0; off >= 1; off >>= 1, ++b)
-            if (lane & off) colbits |= (kH >> (b + 1));
-        atomicAdd(&p.gmlp.weight[2][colbits], gw2a);
-        atomicAdd(&p.gmlp.weight[2][colbits + 1], gw2b);
-        if (lane == 0) atomicAdd(&p.gmlp.bias[2][0], gb2);
+            if (lane & off) colbits |= (32 >> (b + 1));
+        atomicAdd(&p.gmlp.weight[2][col0 + colbits], gw2);
+        if (grp == 0 && lane == 0) atomicAdd(&p.gmlp.bias[2][0], gb2);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -800,7 +868,8 @@ static int max_optin()
     return v;
 }
 
-static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cudaStream_t st)
+static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cudaStream_t st,
+                     int threads = tcf::kThreadsTC)
 {
     const int smem = (int)tcf::TCSmem(p.plane_off[3], bwd).total;
     if (smem > max_optin()) return ATDF_ERR_UNSUPPORTED;
@@ -812,7 +881,7 @@ static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cu
     int dev = 0, sms = 0, per = 0;
     ATDF_CUDA_TRY(cudaGetDevice(&dev));
     ATDF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    ATDF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, tcf::kThreadsTC, smem));
+    ATDF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, threads, smem));
     if (per < 1) return ATDF_ERR_UNSUPPORTED;
     // TMEM: 256 columns per forward CTA, 512 per backward CTA (512 per SM).
     // The forward fits two CTAs per SM by shared memory and registers
@@ -820,12 +889,16 @@ static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cu
     int smem_sm = 0;
     ATDF_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     per = bwd ? 1 : std::max(1, std::min(2, smem_sm / (smem + 1024)));
-    fn<<<sms * per, tcf::kThreadsTC, smem, st>>>(p);
+    fn<<<sms * per, threads, smem, st>>>(p);
     ATDF_LAUNCH_CHECK();
     return ATDF_OK;
 }
 
 int launch_tc_forward(const FusedParams& p, cudaStream_t st) { return launch_tc(tcf::tc_forward_kernel, false, p, st); }
-int launch_tc_backward(const FusedParams& p, cudaStream_t st) { return launch_tc(tcf::tc_backward_kernel, true, p, st); }
+// The backward runs two threads per sample row (512 threads per CTA).
+int launch_tc_backward(const FusedParams& p, cudaStream_t st)
+{
+    return launch_tc(tcf::tc_backward2_kernel, true, p, st, tcf::kThreadsB2);
+}
 
 }  // namespace atdf
