@@ -362,11 +362,14 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
     constexpr int F = K::F, CPT = K::CPT, NF = MODE ? 3 * CPT : CPT;
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_ctl[4];
+    __shared__ int s_ctl[8];
     const Smem<C, MODE, H, NH, false> L(p.plane_off[3]);
     const int tid = threadIdx.x;
     const int s = tid / kSPT, q = tid % kSPT;
-    if (tid == 0) mbar_init(&bar, 1);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        init_item_queue(s_ctl);
+    }
     load_weights<C, MODE, H, NH, false>(p, sm, L);
     __syncthreads();
     SegTab tab = seg_tab(sm + L.segi);
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
         const ItemInfo it = next_item(p, 0, sm, tab, &bar, s_ctl, false);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
-        if (real) {
+        if (real && it.first) {
             if (!mbar_wait(&bar, phase)) {
                 set_err(p.err, ATDF_DEVERR_TREE);
                 mbar_wait(&bar, phase);
@@ -450,12 +453,15 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
     constexpr int F = K::F, CPT = K::CPT, NF = MODE ? 3 * CPT : CPT;
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_ctl[4];
+    __shared__ int s_ctl[8];
     __shared__ int s_lo[3];
     const Smem<C, MODE, H, NH, true> L(p.plane_off[3]);
     const int tid = threadIdx.x;
     const int s = tid / kSPT, q = tid % kSPT;
-    if (tid == 0) mbar_init(&bar, 1);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        init_item_queue(s_ctl);
+    }
     load_weights<C, MODE, H, NH, true>(p, sm, L);
     __syncthreads();
     SegTab tab = seg_tab(sm + L.segi);
@@ -479,8 +485,8 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
         const ItemInfo it = next_item(p, 1, sm, tab, &bar, s_ctl, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
-        // zero the slot's gradient copy and set up the line windows
-        if (real) {
+        // a slot's first item: zero its gradient copy, set up the line windows
+        if (real && it.first) {
             for (int i = tid * 4; i < plane_floats; i += kThreads * 4)
                 *reinterpret_cast<float4*>(sm + L.gplanes + i) = make_float4(0.f, 0.f, 0.f, 0.f);
             for (int i = tid; i < 3 * kLineWin * C; i += kThreads) sm[L.gline + i] = 0.0f;
@@ -669,16 +675,15 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
             }
             __syncthreads();
         }
-        // flush the slot's plane gradients and the line windows
-        if (real) {
+        // a slot's last item: store its plane gradients (this CTA owns the
+        // slot) and flush the line windows
+        if (real && it.last) {
             for (int m = 0; m < 3; ++m) {
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
                 const float* src = sm + L.gplanes + p.plane_off[m];
-                for (int i = tid * 4; i < pf; i += kThreads * 4) {
-                    const float4 v = *reinterpret_cast<const float4*>(src + i);
-                    atomicAdd(reinterpret_cast<float4*>(dst + i), v);
-                }
+                for (int i = tid * 4; i < pf; i += kThreads * 4)
+                    *reinterpret_cast<float4*>(dst + i) = *reinterpret_cast<const float4*>(src + i);
                 const int Ln = p.field.line_len[m];
                 const int lo = s_lo[m];
                 for (int i = tid; i < kLineWin * C; i += kThreads) {

@@ -215,8 +215,9 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
     return t;
 }
 
-// Takes the next work item; fills the segment table; issues the plane TMA.
-// Returns the item's slot, or -1 when the queue is empty.
+// Takes the next work item; fills the segment table; issues the plane TMA
+// when the item starts a new slot. Returns the item's slot, or -1 when the
+// queue is empty.
 // A work item's samples are visited in the order k -> k * 104729 mod total
 // (a permutation: the prime exceeds any item's sample count). Consecutive
 // samples, which share a warp, then come from different rays and depths in
@@ -229,6 +230,8 @@ struct ItemInfo {
     int nseg;
     int total;
     double inv_total;  // 1 / total (for the sample permutation)
+    bool first;        // first item of its slot: the slot's planes were just requested
+    bool last;         // last item of its slot
 };
 
 // (k * kSamplePermPrime) mod total without a 64-bit integer division: the
@@ -246,29 +249,43 @@ __device__ __forceinline__ int perm_index(int k, int total, double inv_total)
     return (int)r;
 }
 
+// Work is handed out by leaf slot: a CTA takes the next slot with segments
+// from the queue (counters[queue] counts slots) and then walks that slot's
+// work items of up to kSegItem segments itself, so each slot's planes are
+// staged once and its gradient copy is zeroed and written back once, by one
+// CTA, with plain stores. s_ctl[4..6] hold the CTA's current slot and its
+// next / end item (thread 0 only; init_item_queue sets them).
+__device__ __forceinline__ void init_item_queue(int* s_ctl)
+{
+    s_ctl[4] = -1;
+    s_ctl[5] = 0;
+    s_ctl[6] = 0;
+}
+
 __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, float* sm, SegTab tab, uint64_t* bar,
                                               int* s_ctl, bool want_dI)
 {
     const Ws& w = p.ws;
     const int tid = threadIdx.x;
     if (tid == 0) {
-        const int nitems = w.item_offset[w.nslot + 1];
-        const int it = atomicAdd(&w.counters[queue], 1);
-        int slot = -1, b0 = 0, nseg = 0;
-        if (it < nitems) {
-            int lo = 0, hi = (int)w.nslot + 1;  // item_offset[lo] <= it < item_offset[hi]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (w.item_offset[mid] <= it)
-                    lo = mid;
-                else
-                    hi = mid;
+        int slot = -1, b0 = 0, nseg = 0, flags = 0;
+        if (s_ctl[5] >= s_ctl[6]) {  // the current slot is done: take the next one with work
+            const int nslots = (int)w.nslot + 1;  // plane slots + the out-of-ROI bucket
+            s_ctl[4] = -1;
+            while (true) {
+                const int sl = atomicAdd(&w.counters[queue], 1);
+                if (sl >= nslots) break;
+                const int i0 = w.item_offset[sl], i1 = w.item_offset[sl + 1];
+                if (i1 > i0) {
+                    s_ctl[4] = sl;
+                    s_ctl[5] = i0;
+                    s_ctl[6] = i1;
+                    flags |= 1;
+                    break;
+                }
             }
-            slot = lo;
-            b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * kSegItem;
-            const int b1 = min(b0 + kSegItem, w.slot_offset[slot + 1]);
-            nseg = b1 - b0;
-            if (slot < w.nslot) {
+            if (s_ctl[4] >= 0 && s_ctl[4] < w.nslot) {
+                const int64_t sl = s_ctl[4];
                 // plane_off counts elements of the plane type (4 or 2 bytes)
                 const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
                 uint32_t bytes = 0;
@@ -279,19 +296,30 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
                 for (int m = 0; m < 3; ++m) {
                     const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
                     tma_bulk_load(reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz,
-                                  reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)slot * pf * esz,
+                                  reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz,
                                   (uint32_t)(pf * esz), bar);
                 }
             }
         }
+        if (s_ctl[4] >= 0 && s_ctl[5] < s_ctl[6]) {
+            slot = s_ctl[4];
+            const int it = s_ctl[5]++;
+            b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * kSegItem;
+            const int b1 = min(b0 + kSegItem, w.slot_offset[slot + 1]);
+            nseg = b1 - b0;
+            if (s_ctl[5] == s_ctl[6]) flags |= 2;
+        }
         s_ctl[0] = slot;
         s_ctl[1] = b0;
         s_ctl[2] = nseg;
+        s_ctl[3] = flags;
     }
     __syncthreads();
     ItemInfo info;
     info.slot = s_ctl[0];
     info.nseg = s_ctl[2];
+    info.first = (s_ctl[3] & 1) != 0;
+    info.last = (s_ctl[3] & 2) != 0;
     info.total = 0;
     info.inv_total = 0.0;
     if (info.slot < 0) return info;

@@ -292,12 +292,13 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
     __shared__ __align__(8) uint64_t bar_tma;
     __shared__ __align__(8) uint64_t bar_mma[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_ctl[4];
+    __shared__ int s_ctl[8];
     const TCSmem L(p.plane_off[3], false);
     const int tid = threadIdx.x, h = tid / kRows, t = tid % kRows;
     if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemFwd);
     if (tid == 0) {
         mbar_init(&bar_tma, 1);
+        init_item_queue(s_ctl);
         mbar_init(&bar_mma[0], 1);
         mbar_init(&bar_mma[1], 1);
     }
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
         const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
-        if (real) {
+        if (real && it.first) {
             if (!mbar_wait(&bar_tma, tma_phase)) {
                 set_err(p.err, ATDF_DEVERR_TREE);
                 mbar_wait(&bar_tma, tma_phase);
@@ -467,7 +468,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     __shared__ __align__(8) uint64_t bar_tma;
     __shared__ __align__(8) uint64_t bar_mma[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_ctl[4];
+    __shared__ int s_ctl[8];
     __shared__ int s_lo[3];
     __shared__ float s_z[2][2][kRows];  // partial last-layer sums [half][group][row]
     const TCSmem L(p.plane_off[3], true);
@@ -478,6 +479,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemBwd);
     if (tid == 0) {
         mbar_init(&bar_tma, 1);
+        init_item_queue(s_ctl);
         mbar_init(&bar_mma[0], 1);
         mbar_init(&bar_mma[1], 1);
     }
@@ -514,7 +516,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
         const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
-        if (real) {
+        if (real && it.first) {
             for (int i = tid * 4; i < plane_elems; i += kThreadsB2 * 4)
                 *reinterpret_cast<float4*>(gpl + i) = make_float4(0.f, 0.f, 0.f, 0.f);
             for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsB2) gln[i] = 0.0f;
@@ -795,13 +797,13 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             half_barrier2(h);
         }
         alive = __syncthreads_and(alive);
-        if (real) {
+        if (real && it.last) {  // this CTA owns the slot: plain stores
             for (int m = 0; m < 3; ++m) {
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
                 const float* src = gpl + p.plane_off[m];
                 for (int i = tid * 4; i < pf; i += kThreadsB2 * 4)
-                    atomicAdd(reinterpret_cast<float4*>(dst + i), *reinterpret_cast<const float4*>(src + i));
+                    *reinterpret_cast<float4*>(dst + i) = *reinterpret_cast<const float4*>(src + i);
                 const int Ln = p.field.line_len[m];
                 const int lo = s_lo[m];
                 for (int i = tid; i < kLineWinTC * C; i += kThreadsB2) {
