@@ -826,15 +826,24 @@ static int prepare(const atdf_tree_t* tree, const atdf_field_t* field, const atd
     }
     for (int l = 0; l < mlp->num_layers; ++l)
         if (!mlp->weight[l] || !mlp->bias[l]) return ATDF_ERR_INVALID_ARGUMENT;
-    int off = 0;
+    // The BF16 tensor-core kernels keep each plane in shared memory with rows
+    // padded to a pitch of 2 mod 4 texels (texel = 16 channels = 32 bytes):
+    // the four corners of a bilinear footprint then have texel indices of
+    // all four residues mod 4 and fill distinct bank groups.
+    int off = 0, goff = 0;
     for (int m = 0; m < 3; ++m) {
         if (!field->plane[m] || !field->line[m] || ((uintptr_t)field->plane[m] & 15) ||
             ((uintptr_t)field->line[m] & 15))
             return ATDF_ERR_UNSUPPORTED;
+        const int W = field->plane_w[m];
+        p.plane_pitch[m] = field->dtype == ATDF_BF16 ? W + ((2 - W) & 3) : W;
         p.plane_off[m] = off;
-        off += field->plane_h[m] * field->plane_w[m] * field->channels;
+        off += field->plane_h[m] * p.plane_pitch[m] * field->channels;
+        p.gplane_off[m] = goff;
+        goff += field->plane_h[m] * W * field->channels;
     }
     p.plane_off[3] = off;
+    p.gplane_off[3] = goff;
     p.roi_inv = pow2_reciprocal(field->roi_max[0] - field->roi_min[0]);
     const size_t need = ws_layout(R, tree->max_depth, field->num_slots, nullptr, nullptr);
     if (ws_bytes < need) return ATDF_ERR_WORKSPACE;

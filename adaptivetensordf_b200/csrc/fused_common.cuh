@@ -161,7 +161,9 @@ struct FusedParams {
     atdf_field_grad_t gfield;
     atdf_mlp_grad_t gmlp;
     int32_t* err;
-    int plane_off[4];  // float offsets of the three planes in shared memory (+ total)
+    int plane_off[4];    // element offsets of the three planes in shared memory (+ total)
+    int plane_pitch[3];  // texels per shared-memory row of each plane (>= plane_w)
+    int gplane_off[4];   // float offsets of the unpadded FP32 plane-gradient copy (+ total)
     float roi_inv;     // 1 / (roi_max.x - roi_min.x) when a power of two, else 0
     // Caller-placed samples (null: the uniform per-node rule): t and weight
     // of every sample in canonical order, indexed by the ray's sample offset
@@ -295,9 +297,16 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
                 mbar_expect_tx(bar, bytes);
                 for (int m = 0; m < 3; ++m) {
                     const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
-                    tma_bulk_load(reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz,
-                                  reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz,
-                                  (uint32_t)(pf * esz), bar);
+                    char* dst = reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz;
+                    const char* src = reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz;
+                    if (p.plane_pitch[m] == p.field.plane_w[m]) {
+                        tma_bulk_load(dst, src, (uint32_t)(pf * esz), bar);
+                    } else {  // padded rows: one copy per row
+                        const uint32_t row = (uint32_t)(p.field.plane_w[m] * p.field.channels * esz);
+                        const uint32_t pitch = (uint32_t)(p.plane_pitch[m] * p.field.channels * esz);
+                        for (int r = 0; r < p.field.plane_h[m]; ++r)
+                            tma_bulk_load(dst + (size_t)r * pitch, src + (size_t)r * row, row, bar);
+                    }
                 }
             }
         }

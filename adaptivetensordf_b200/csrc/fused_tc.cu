@@ -50,7 +50,7 @@ __device__ __forceinline__ uint32_t w1_off(int n, int k) { return tc::kmajor_off
 
 struct TCSmem {
     uint32_t planes, w0, w1, bias, hb[2], g[2], gplanes, gline, sw[2], sdi[2], sseg[2], segi, total;
-    __host__ __device__ TCSmem(int plane_elems, bool bwd)
+    __host__ __device__ TCSmem(int plane_elems, int gplane_elems, bool bwd)
     {
         auto al = [](uint32_t x) { return (x + 127u) & ~127u; };
         uint32_t o = 0;
@@ -71,7 +71,7 @@ struct TCSmem {
             if (bwd) o = al(o + kRows * kGCols * 2);
         }
         gplanes = o;
-        if (bwd) o = al(o + plane_elems * 4);
+        if (bwd) o = al(o + gplane_elems * 4);
         gline = o;
         if (bwd) o = al(o + 3 * kLineWinTC * kC * 4);
         for (int h = 0; h < 2; ++h) {
@@ -157,43 +157,71 @@ __device__ __forceinline__ void ld16(const float* src, float (&v)[16])
     }
 }
 
-// VM feature of one sample (16 channels) from the BF16 planes in shared
-// memory and the BF16 lines in global memory.
-__device__ __forceinline__ void gather_features(const FusedParams& p, const unsigned char* sm, const SampleGeo& g,
-                                                float (&f)[kC], float (&mat)[3][kC], float (&vec)[3][kC])
+// Texel index (padded rows of pitch Wp) and weight of corner o of a bilinear
+// footprint: 0 = (y0, x0), 1 = (y0, x1), 2 = (y1, x0), 3 = (y1, x1).
+__device__ __forceinline__ int corner_texel(const Corner2& k, int o, int Wp, float& w)
 {
+    w = o == 0 ? k.w_nw : (o == 1 ? k.w_ne : (o == 2 ? k.w_sw : k.w_se));
+    return ((o & 2) ? k.y1 : k.y0) * Wp + ((o & 1) ? k.x1 : k.x0);
+}
+
+// Corner visited first by this lane. A texel (16 BF16 channels) spans two
+// 16-byte bank groups, and with the pitch at 2 mod 4 the corners' texel
+// indices are r, r + 1, r + 2, r + 3 mod 4 (r of corner 0), so the 8
+// (corner, half) chunks of a footprint fill all 8 groups of a 128-byte bank
+// row. 16-byte loads are served per 8-lane phase; lane p of a phase starts
+// at the corner of residue sel(p) and walks the corners in residue order,
+// which spreads one instruction's loads of the phase over distinct groups.
+__device__ __forceinline__ int first_corner(const Corner2& k, int Wp, int sel)
+{
+    return (sel - (k.y0 * Wp + k.x0)) & 3;
+}
+
+// VM feature of one sample (16 channels) from the BF16 planes in shared
+// memory (padded rows) and the BF16 lines in global memory: fa = channels
+// 8 * hf .. 8 * hf + 7, fb = the other eight, hf = lane mod 2. Lane p of an
+// 8-lane phase loads at step j the corner of residue p / 2 + j, first half
+// hf, then half 1 - hf: 8 distinct bank groups per instruction and phase.
+__device__ __forceinline__ void gather_features(const FusedParams& p, const unsigned char* sm, const SampleGeo& g,
+                                                float (&fa)[8], float (&fb)[8])
+{
+    const int lane = threadIdx.x & 31, hf = lane & 1;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 2; m >= 0; --m) {
         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
+        const int Wp = p.plane_pitch[m];
         const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
         const Corner1 l = corners1(g.lu[m], L);
         const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
         const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
+        const int c0 = first_corner(k, Wp, (lane & 7) >> 1);
+        float ma[8], mb[8];
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            float a[8], b[8], c[8], d[8], v0[8], v1[8];
-            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x0) * kC + 8 * half) * 2), a);
-            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x1) * kC + 8 * half) * 2), b);
-            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x0) * kC + 8 * half) * 2), c);
-            unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x1) * kC + 8 * half) * 2), d);
-            unpack_bf16x8(__ldg(V + l.x0 * 2 + half), v0);
-            unpack_bf16x8(__ldg(V + l.x1 * 2 + half), v1);
+        for (int j = 0; j < 4; ++j) {
+            float w;
+            const unsigned char* tx = P + corner_texel(k, (c0 + j) & 3, Wp, w) * (kC * 2);
+            float u[8], v[8];
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(tx + 16 * hf), u);
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(tx + 16 * (hf ^ 1)), v);
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const int ch = 8 * half + i;
-                float acc = a[i] * k.w_nw;
-                acc = fmaf(b[i], k.w_ne, acc);
-                acc = fmaf(c[i], k.w_sw, acc);
-                acc = fmaf(d[i], k.w_se, acc);
-                mat[m][ch] = acc;
-                vec[m][ch] = fmaf(v0[i], l.w0, v1[i] * l.w1);
+                ma[i] = j == 0 ? u[i] * w : fmaf(u[i], w, ma[i]);
+                mb[i] = j == 0 ? v[i] * w : fmaf(v[i], w, mb[i]);
             }
         }
-    }
+        float va0[8], va1[8], vb0[8], vb1[8];
+        unpack_bf16x8(__ldg(V + l.x0 * 2 + hf), va0);
+        unpack_bf16x8(__ldg(V + l.x1 * 2 + hf), va1);
+        unpack_bf16x8(__ldg(V + l.x0 * 2 + (hf ^ 1)), vb0);
+        unpack_bf16x8(__ldg(V + l.x1 * 2 + (hf ^ 1)), vb1);
 #pragma unroll
-    for (int ch = 0; ch < kC; ++ch) f[ch] = fmaf(mat[0][ch], vec[0][ch], fmaf(mat[1][ch], vec[1][ch], mat[2][ch] * vec[2][ch]));
+        for (int i = 0; i < 8; ++i) {
+            const float vea = fmaf(va0[i], l.w0, va1[i] * l.w1), veb = fmaf(vb0[i], l.w0, vb1[i] * l.w1);
+            fa[i] = m == 2 ? ma[i] * vea : fmaf(ma[i], vea, fa[i]);
+            fb[i] = m == 2 ? mb[i] * veb : fmaf(mb[i], veb, fb[i]);
+        }
+    }
 }
-
 
 __device__ __forceinline__ void load_weights_tc(const FusedParams& p, unsigned char* sm, const TCSmem& L)
 {
@@ -247,9 +275,9 @@ __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned cha
                                               int t, float& w, int& si, SampleGeo& g, float& ts)
 {
     const bool valid = k < it.total;
-    float f[kC];
+    float fa[8], fb[8];
 #pragma unroll
-    for (int i = 0; i < kC; ++i) f[i] = 0.0f;
+    for (int i = 0; i < 8; ++i) fa[i] = fb[i] = 0.0f;
     w = 0.0f;
     ts = 0.0f;
     si = -1;
@@ -260,12 +288,12 @@ __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned cha
         si = st.si;
         if (real) {
             g = sample_geo_fast(p, tab, st.si, st.pos);
-            float mat[3][kC], vec[3][kC];
-            gather_features(p, sm, g, f, mat, vec);
+            gather_features(p, sm, g, fa, fb);
         }
     }
-    store_bf16x8(sm + L.hb[h] + hb_off(t, kH), f);
-    store_bf16x8(sm + L.hb[h] + hb_off(t, kH + 8), f + 8);
+    const int hf = threadIdx.x & 1;
+    store_bf16x8(sm + L.hb[h] + hb_off(t, kH + 8 * hf), fa);
+    store_bf16x8(sm + L.hb[h] + hb_off(t, kH + 8 * (hf ^ 1)), fb);
     return valid;
 }
 
@@ -293,7 +321,7 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
     __shared__ __align__(8) uint64_t bar_mma[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_ctl[8];
-    const TCSmem L(p.plane_off[3], false);
+    const TCSmem L(p.plane_off[3], p.gplane_off[3], false);
     const int tid = threadIdx.x, h = tid / kRows, t = tid % kRows;
     if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemFwd);
     if (tid == 0) {
@@ -395,31 +423,32 @@ constexpr int kThreadsB2 = 512;
 __device__ __forceinline__ void half_barrier2(int h) { asm volatile("bar.sync %0, 256;" ::"r"(1 + h) : "memory"); }
 
 // Bilinear plane values and linear line values of plane / line m for the 8
-// channels cb..cb+7 of one sample.
+// channels cb..cb+7 of one sample (cb is the same across a warp, so one
+// 8-lane phase can reach 4 of the 8 bank groups: lanes p and p + 4 of a
+// phase share a corner residue, two loads per group).
 __device__ __forceinline__ void gather_half(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
                                             int cb, float (&mat)[8], float (&vec)[8])
 {
     const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
+    const int Wp = p.plane_pitch[m];
     const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
     const Corner1 l = corners1(g.lu[m], L);
-    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
+    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2 + cb * 2;
     const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
-    float a[8], b[8], c[8], d[8], v0[8], v1[8];
-    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x0) * kC + cb) * 2), a);
-    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y0 * Wm + k.x1) * kC + cb) * 2), b);
-    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x0) * kC + cb) * 2), c);
-    unpack_bf16x8(*reinterpret_cast<const uint4*>(P + ((k.y1 * Wm + k.x1) * kC + cb) * 2), d);
+    const int c0 = first_corner(k, Wp, threadIdx.x & 3);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float w, u[8];
+        const int tx = corner_texel(k, (c0 + j) & 3, Wp, w);
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + tx * (kC * 2)), u);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) mat[i] = j == 0 ? u[i] * w : fmaf(u[i], w, mat[i]);
+    }
+    float v0[8], v1[8];
     unpack_bf16x8(__ldg(V + l.x0 * 2 + (cb >> 3)), v0);
     unpack_bf16x8(__ldg(V + l.x1 * 2 + (cb >> 3)), v1);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        float acc = a[i] * k.w_nw;
-        acc = fmaf(b[i], k.w_ne, acc);
-        acc = fmaf(c[i], k.w_sw, acc);
-        acc = fmaf(d[i], k.w_se, acc);
-        mat[i] = acc;
-        vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
-    }
+    for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
 }
 
 // Features (channels cb..cb+7) of tile row t into HB; returns validity.
@@ -439,7 +468,7 @@ __device__ __forceinline__ bool tile_features_half(const FusedParams& p, unsigne
         si = st.si;
         if (real) {
             g = sample_geo_fast(p, tab, st.si, st.pos);
-            // planes 2, 1, 0: the same operation order as gather_features
+            // planes 2, 1, 0, as in gather_features
 #pragma unroll
             for (int m = 2; m >= 0; --m) {
                 float mat[8], vec[8];
@@ -471,7 +500,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     __shared__ int s_ctl[8];
     __shared__ int s_lo[3];
     __shared__ float s_z[2][2][kRows];  // partial last-layer sums [half][group][row]
-    const TCSmem L(p.plane_off[3], true);
+    const TCSmem L(p.plane_off[3], p.gplane_off[3], true);
     const int tid = threadIdx.x, h = tid >> 8, grp = (tid >> 7) & 1, t = tid & (kRows - 1), lane = tid & 31;
     const int cb = 8 * grp;       // channels of this group
     const int col0 = 32 * grp;    // hidden columns of this group
@@ -503,7 +532,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     const float beta = p.mlp.softplus_beta;
     const int lact = p.mlp.last_activation;
     const int C = kC;
-    const int plane_elems = p.plane_off[3];
+    const int gplane_elems = p.gplane_off[3];
     float* gpl = reinterpret_cast<float*>(sm + L.gplanes);
     float* gln = reinterpret_cast<float*>(sm + L.gline);
     unsigned char* hbh = sm + L.hb[h];
@@ -511,13 +540,13 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true, had_tile = false;
     float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group
-    const int rot = lane + (lane >> 3);
+    const int crot = 2 * (lane & 7) + ((lane >> 3) & 1) + 2 * (lane >> 4);
     while (alive) {
         const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {
-            for (int i = tid * 4; i < plane_elems; i += kThreadsB2 * 4)
+            for (int i = tid * 4; i < gplane_elems; i += kThreadsB2 * 4)
                 *reinterpret_cast<float4*>(gpl + i) = make_float4(0.f, 0.f, 0.f, 0.f);
             for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsB2) gln[i] = 0.0f;
             if (tid < 3) {
@@ -756,21 +785,31 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                     }
                     tc::commit(&bar_mma[h]);
                 }
-                // scatter, phase 2: plane gradients, 16 channels in lane-rotated
-                // order (different banks per lane); group 0 adds the two upper
-                // corners, group 1 the two lower ones
+                // scatter, phase 2: plane gradients; group 0 adds the two upper
+                // corners, group 1 the two lower ones. A texel's 16 FP32
+                // channels fill one half of the 32 banks (the half given by the
+                // parity of its index), and the two corners of a row have
+                // opposite parities: lanes 0-15 take first the corner in banks
+                // 0-15, lanes 16-31 the one in banks 16-31, and channel
+                // (r + crot) mod 16 with crot a permutation of 0..15 within
+                // each half-warp, so every warp-wide atomic touches 32 distinct
+                // banks. crot mod 4 also differs among the four lanes that share
+                // lane mod 8, which keeps the scratch-row reads conflict-free.
                 if (valid) {
 #pragma unroll 1
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
                         const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
-                        float* GP = gpl + p.plane_off[m];
+                        float* GP = gpl + p.gplane_off[m];
                         const int ya = grp == 0 ? kc.y0 : kc.y1;
-                        const float wa = grp == 0 ? kc.w_nw : kc.w_sw, wb = grp == 0 ? kc.w_ne : kc.w_se;
-                        const int ta = (ya * Wm + kc.x0) * C, tb = (ya * Wm + kc.x1) * C;
+                        const float wl = grp == 0 ? kc.w_nw : kc.w_sw, wr = grp == 0 ? kc.w_ne : kc.w_se;
+                        const int tl = ya * Wm + kc.x0, tr = ya * Wm + kc.x1;
+                        const bool swap = (tl & 1) != (lane >> 4);
+                        const int ta = (swap ? tr : tl) * C, tb = (swap ? tl : tr) * C;
+                        const float wa = swap ? wr : wl, wb = swap ? wl : wr;
 #pragma unroll 4
                         for (int r = 0; r < kC; ++r) {
-                            const int c = (r + rot) & (kC - 1);
+                            const int c = (r + crot) & (kC - 1);
                             const float v = *scratch2(hbh, gh, t, 16 * m + c);
                             atomicAdd(&GP[ta + c], wa * v);
                             atomicAdd(&GP[tb + c], wb * v);
@@ -801,7 +840,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             for (int m = 0; m < 3; ++m) {
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
-                const float* src = gpl + p.plane_off[m];
+                const float* src = gpl + p.gplane_off[m];
                 for (int i = tid * 4; i < pf; i += kThreadsB2 * 4)
                     *reinterpret_cast<float4*>(dst + i) = *reinterpret_cast<const float4*>(src + i);
                 const int Ln = p.field.line_len[m];
@@ -873,7 +912,7 @@ static int max_optin()
 static int launch_tc(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cudaStream_t st,
                      int threads = tcf::kThreadsTC)
 {
-    const int smem = (int)tcf::TCSmem(p.plane_off[3], bwd).total;
+    const int smem = (int)tcf::TCSmem(p.plane_off[3], p.gplane_off[3], bwd).total;
     if (smem > max_optin()) return ATDF_ERR_UNSUPPORTED;
     ATDF_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     // without an explicit carveout the occupancy query assumes a smaller
