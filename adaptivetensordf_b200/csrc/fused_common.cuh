@@ -234,6 +234,7 @@ struct ItemInfo {
     double inv_total;  // 1 / total (for the sample permutation)
     bool first;        // first item of its slot: the slot's planes were just requested
     bool last;         // last item of its slot
+    int slot_items;    // work items of the slot
 };
 
 // (k * kSamplePermPrime) mod total without a 64-bit integer division: the
@@ -256,12 +257,14 @@ __device__ __forceinline__ int perm_index(int k, int total, double inv_total)
 // work items of up to kSegItem segments itself, so each slot's planes are
 // staged once and its gradient copy is zeroed and written back once, by one
 // CTA, with plain stores. s_ctl[4..6] hold the CTA's current slot and its
-// next / end item (thread 0 only; init_item_queue sets them).
+// next / end item (thread 0 only; init_item_queue sets them), s_ctl[7] the
+// slot's item count.
 __device__ __forceinline__ void init_item_queue(int* s_ctl)
 {
     s_ctl[4] = -1;
     s_ctl[5] = 0;
     s_ctl[6] = 0;
+    s_ctl[7] = 0;
 }
 
 __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, float* sm, SegTab tab, uint64_t* bar,
@@ -282,6 +285,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
                     s_ctl[4] = sl;
                     s_ctl[5] = i0;
                     s_ctl[6] = i1;
+                    s_ctl[7] = i1 - i0;
                     flags |= 1;
                     break;
                 }
@@ -329,6 +333,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     info.nseg = s_ctl[2];
     info.first = (s_ctl[3] & 1) != 0;
     info.last = (s_ctl[3] & 2) != 0;
+    info.slot_items = s_ctl[7];
     info.total = 0;
     info.inv_total = 0.0;
     if (info.slot < 0) return info;

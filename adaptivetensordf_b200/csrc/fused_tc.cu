@@ -500,6 +500,11 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     __shared__ int s_ctl[8];
     __shared__ int s_lo[3];
     __shared__ float s_z[2][2][kRows];  // partial last-layer sums [half][group][row]
+    // fixed-point plane-gradient accumulation of the current slot
+    __shared__ float s_tcum[2];    // per half: sum of |contribution| over the slot's tiles so far
+    __shared__ float s_tfirst[2];  // per half: the same over its first tile (scale choice)
+    __shared__ float s_scale;      // the slot's scale (a power of two; 0 = not chosen yet)
+    __shared__ int s_fb;           // a tile of the slot went to global memory in FP32
     const TCSmem L(p.plane_off[3], p.gplane_off[3], true);
     const int tid = threadIdx.x, h = tid >> 8, grp = (tid >> 7) & 1, t = tid & (kRows - 1), lane = tid & 31;
     const int cb = 8 * grp;       // channels of this group
@@ -533,7 +538,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     const int lact = p.mlp.last_activation;
     const int C = kC;
     const int gplane_elems = p.gplane_off[3];
-    float* gpl = reinterpret_cast<float*>(sm + L.gplanes);
+    int* gpl = reinterpret_cast<int*>(sm + L.gplanes);  // the slot's plane gradients, fixed point
     float* gln = reinterpret_cast<float*>(sm + L.gline);
     unsigned char* hbh = sm + L.hb[h];
     unsigned char* gh = sm + L.g[h];
@@ -541,13 +546,23 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     bool alive = true, had_tile = false;
     float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group
     const int crot = 2 * (lane & 7) + ((lane >> 3) & 1) + 2 * (lane >> 4);
+    float scale = 0.f;  // the slot's fixed-point scale
+    int ntiles = 0;     // tiles of this half in the slot
     while (alive) {
         const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {
             for (int i = tid * 4; i < gplane_elems; i += kThreadsB2 * 4)
-                *reinterpret_cast<float4*>(gpl + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+                *reinterpret_cast<int4*>(gpl + i) = make_int4(0, 0, 0, 0);
+            if (tid == 0) {
+                s_tcum[0] = s_tcum[1] = 0.f;
+                s_tfirst[0] = s_tfirst[1] = 0.f;
+                s_scale = 0.f;
+                s_fb = 0;
+            }
+            scale = 0.f;
+            ntiles = 0;
             for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsB2) gln[i] = 0.0f;
             if (tid < 3) {
                 float bmin[3], bmax[3];
@@ -570,7 +585,14 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             tma_phase ^= 1;
         }
         alive = __syncthreads_and(alive);
+        // The scale is chosen once per slot, at the first tile of each half
+        // (both halves together when the item gives both a tile), from the
+        // measured contributions of those tiles; later items read it.
+        const bool scale_set = s_scale != 0.f;
+        if (scale_set) scale = s_scale;
+        const bool both = it.total > kRows;
         for (int t0 = h * kRows; alive && t0 < it.total; t0 += 2 * kRows) {
+            const bool handshake = !scale_set && t0 == h * kRows;
             SampleGeo g;
             float w;
             int si;
@@ -732,17 +754,22 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
 #pragma unroll
                     for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(gh + g_off(t, 8 * q)) = z4;
                 }
+                float tsum = 0.f;  // sum of |dX * line value| of this thread's 24 values
                 if (valid) {
 #pragma unroll 1
                     for (int m = 0; m < 3; ++m) {
                         const int Ln = p.field.line_len[m];
-                        float mat[8], vec[8], lv[8];
+                        float mat[8], vec[8], lv[8], gv[8];
                         gather_half(p, sm, g, m, cb, mat, vec);
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            gv[c] = dx[c] * vec[c];
+                            tsum += fabsf(gv[c]);
+                        }
 #pragma unroll
                         for (int q = 0; q < 2; ++q)
                             *reinterpret_cast<float4*>(scratch2(hbh, gh, t, 16 * m + cb + 4 * q)) =
-                                make_float4(dx[4 * q] * vec[4 * q], dx[4 * q + 1] * vec[4 * q + 1],
-                                            dx[4 * q + 2] * vec[4 * q + 2], dx[4 * q + 3] * vec[4 * q + 3]);
+                                make_float4(gv[4 * q], gv[4 * q + 1], gv[4 * q + 2], gv[4 * q + 3]);
 #pragma unroll
                         for (int c = 0; c < 8; ++c) lv[c] = dx[c] * mat[c];
                         store_bf16x8(hbh + hb_off(t, 16 * m + cb), lv);
@@ -769,9 +796,38 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                         }
                     }
                 }
+                // The bilinear weights of a sample sum to 1, so the tile adds at
+                // most sum |dX * line value| to any texel of the slot.
+#pragma unroll
+                for (int off = 16; off >= 1; off >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, off);
+                if (lane == 0) {
+                    atomicAdd(&s_tcum[h], tsum);
+                    if (handshake) atomicAdd(&s_tfirst[h], tsum);
+                }
                 tc::fence_smem_to_async();
                 tc::fence_before_sync();
-                half_barrier2(h);
+                if (handshake && both)
+                    asm volatile("bar.sync 3, 512;" ::: "memory");
+                else
+                    half_barrier2(h);
+                if (handshake) {
+                    // scale = 2^e with the slot's expected total near 2^28 per
+                    // half (the tiles of this half estimated from this item)
+                    const float first = both ? 0.5f * (s_tfirst[0] + s_tfirst[1]) : s_tfirst[0];
+                    const float tiles = fmaxf(1.f, ceilf((float)it.total * (float)it.slot_items / (2.f * kRows)));
+                    int e = 20;
+                    if (first > 0.f) e = ilogbf(268435456.0f / (first * tiles));
+                    scale = ldexpf(1.0f, max(-100, min(e, 100)));
+                    if (tid == 0) s_scale = scale;
+                }
+                // Overflow guard: a half may bring the slot's values at most
+                // to 2^30 in magnitude (sum of its scaled |contributions| plus
+                // half a unit of rounding per contribution); a tile beyond
+                // that goes to global memory in FP32.
+                ++ntiles;
+                const bool to_smem =
+                    s_tcum[h] * scale + (float)ntiles * (0.5f * kRows * 3 * 4 * kC) <= 1073741824.0f;
+                if (!to_smem && issuer) s_fb = 1;
                 if (issuer) {  // line gradients of the tile (overlaps the plane atomics)
                     tc::fence_after_sync();
                     const uint32_t abase = tc::smem_addr(gh), bbase = tc::smem_addr(hbh);
@@ -785,10 +841,11 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                     }
                     tc::commit(&bar_mma[h]);
                 }
-                // scatter, phase 2: plane gradients; group 0 adds the two upper
-                // corners, group 1 the two lower ones. A texel's 16 FP32
-                // channels fill one half of the 32 banks (the half given by the
-                // parity of its index), and the two corners of a row have
+                // scatter, phase 2: plane gradients as fixed-point integers
+                // (shared-memory integer atomics run several times faster than
+                // FP32 ones); group 0 adds the two upper corners, group 1 the
+                // two lower ones. A texel's 16 channels fill one half of the
+                // 32 banks (the half given by the parity of its index), and the two corners of a row have
                 // opposite parities: lanes 0-15 take first the corner in banks
                 // 0-15, lanes 16-31 the one in banks 16-31, and channel
                 // (r + crot) mod 16 with crot a permutation of 0..15 within
@@ -800,19 +857,29 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
                         const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
-                        float* GP = gpl + p.gplane_off[m];
                         const int ya = grp == 0 ? kc.y0 : kc.y1;
                         const float wl = grp == 0 ? kc.w_nw : kc.w_sw, wr = grp == 0 ? kc.w_ne : kc.w_se;
                         const int tl = ya * Wm + kc.x0, tr = ya * Wm + kc.x1;
                         const bool swap = (tl & 1) != (lane >> 4);
                         const int ta = (swap ? tr : tl) * C, tb = (swap ? tl : tr) * C;
                         const float wa = swap ? wr : wl, wb = swap ? wl : wr;
+                        if (to_smem) {
+                            int* GP = gpl + p.gplane_off[m];
+                            const float was = wa * scale, wbs = wb * scale;
 #pragma unroll 4
-                        for (int r = 0; r < kC; ++r) {
-                            const int c = (r + crot) & (kC - 1);
-                            const float v = *scratch2(hbh, gh, t, 16 * m + c);
-                            atomicAdd(&GP[ta + c], wa * v);
-                            atomicAdd(&GP[tb + c], wb * v);
+                            for (int r = 0; r < kC; ++r) {
+                                const int c = (r + crot) & (kC - 1);
+                                const float v = *scratch2(hbh, gh, t, 16 * m + c);
+                                atomicAdd(&GP[ta + c], __float2int_rn(was * v));
+                                atomicAdd(&GP[tb + c], __float2int_rn(wbs * v));
+                            }
+                        } else {
+                            float* GG = p.gfield.plane[m] + it.slot * (int64_t)(Hm * Wm * C);
+                            for (int r = 0; r < kC; ++r) {
+                                const float v = *scratch2(hbh, gh, t, 16 * m + r);
+                                atomicAdd(&GG[ta + r], wa * v);
+                                atomicAdd(&GG[tb + r], wb * v);
+                            }
                         }
                     }
                 }
@@ -836,13 +903,23 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             half_barrier2(h);
         }
         alive = __syncthreads_and(alive);
-        if (real && it.last) {  // this CTA owns the slot: plain stores
+        if (real && it.last) {
+            // this CTA owns the slot: plain stores, unless a tile went to
+            // global memory directly
+            const float sc = s_scale, inv = sc > 0.f ? 1.0f / sc : 0.f;  // exact: a power of two
+            const bool fb = s_fb != 0;
             for (int m = 0; m < 3; ++m) {
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
-                const float* src = gpl + p.gplane_off[m];
-                for (int i = tid * 4; i < pf; i += kThreadsB2 * 4)
-                    *reinterpret_cast<float4*>(dst + i) = *reinterpret_cast<const float4*>(src + i);
+                const int* src = gpl + p.gplane_off[m];
+                for (int i = tid * 4; i < pf; i += kThreadsB2 * 4) {
+                    const int4 q = *reinterpret_cast<const int4*>(src + i);
+                    const float4 v = make_float4((float)q.x * inv, (float)q.y * inv, (float)q.z * inv, (float)q.w * inv);
+                    if (fb)
+                        atomicAdd(reinterpret_cast<float4*>(dst + i), v);
+                    else
+                        *reinterpret_cast<float4*>(dst + i) = v;
+                }
                 const int Ln = p.field.line_len[m];
                 const int lo = s_lo[m];
                 for (int i = tid; i < kLineWinTC * C; i += kThreadsB2) {

@@ -65,3 +65,39 @@ def test_bf16_tensor_core_projection(oracle, depth, R, M, seed_j):
     print("BF16 gradients rel err: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     for k, v in errs.items():
         assert v < BF16_TOL, k
+
+
+def test_bf16_plane_gradient_dynamic_range(oracle):
+    """The tensor-core backward sums each leaf's plane gradients as fixed-point
+    integers with a per-leaf scale chosen from the first tiles, and sends a
+    tile that would exceed the integer range to global memory in FP32. Image
+    gradients spread over twelve decades (random signs) make the tiles of a
+    leaf differ by orders of magnitude, so both paths run; every leaf's plane
+    gradient must still match the oracle to BF16_TOL of its own norm."""
+    import adaptivetensordf_b200 as ab
+
+    depth, R, M, seed_j = 3, 900, 12, 3
+    L = (17 - 1) * (1 << depth)
+    tree, geo, o, d = gpu_scene(depth, 16, 17, (L, 17, L), [64, 64], R, seed=41)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    td, fd, md = oracle_views(tree, geo)
+    fd_b = {**fd, "planes": [_bf16(p) for p in fd["planes"]], "lines": [_bf16(l) for l in fd["lines"]]}
+    md_b = {**md, "layers": [(_bf16(w), b.astype(np.float64)) for w, b in md["layers"]]}
+    md_b["layers"][-1] = (md["layers"][-1][0].astype(np.float64), md["layers"][-1][1].astype(np.float64))
+    rays = ab.RayList(torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda())
+    img = geo.ProjectRays(tree, rays, M, seed_j)
+    rng = np.random.default_rng(12)
+    gi = (10.0 ** rng.uniform(-6, 6, size=(1, R))) * rng.choice([-1.0, 1.0], size=(1, R))
+    img.backward(torch.from_numpy(gi.astype(np.float32)).cuda())
+    segs = oracle.ray_segments(td, o, d, M)
+    so = oracle.emit_samples(segs, o, d, oracle.jitter_for_segments(seed_j, segs))
+    gr = oracle.project_backward(fd_b, md_b, td, so, R, gi.astype(np.float32).astype(np.float64), np.float64)
+    worst = 0.0
+    for m in range(3):
+        got, ref = geo.planes[m].grad.cpu().numpy(), gr["planes"][m]
+        for s in range(ref.shape[0]):
+            if np.abs(ref[s]).max() > 0:
+                worst = max(worst, rel_err(got[s], ref[s]))
+    print(f"\nworst per-leaf plane-gradient rel err over 12 decades of dI: {worst:.2e}")
+    assert worst < BF16_TOL
