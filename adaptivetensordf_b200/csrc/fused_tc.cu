@@ -451,15 +451,32 @@ __device__ __forceinline__ void gather_half(const FusedParams& p, const unsigned
     for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
 }
 
+// Linear line values of line m for the 8 channels cb..cb+7 of one sample.
+__device__ __forceinline__ void line_half(const FusedParams& p, const SampleGeo& g, int m, int cb, float (&vec)[8])
+{
+    const Corner1 l = corners1(g.lu[m], p.field.line_len[m]);
+    const uint4* V = reinterpret_cast<const uint4*>(p.field.line[m]);
+    float v0[8], v1[8];
+    unpack_bf16x8(__ldg(V + l.x0 * 2 + (cb >> 3)), v0);
+    unpack_bf16x8(__ldg(V + l.x1 * 2 + (cb >> 3)), v1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
+}
+
 // Features (channels cb..cb+7) of tile row t into HB; returns validity.
+// The bilinear plane values are kept (as BF16) in 12 TMEM columns at stash
+// for the scatter of the same tile, which then does not gather them again.
 __device__ __forceinline__ bool tile_features_half(const FusedParams& p, unsigned char* sm, const TCSmem& L,
                                                    const SegTab& tab, const ItemInfo& it, bool real, int h, int k,
-                                                   int t, int cb, float& w, int& si, SampleGeo& g)
+                                                   int t, int cb, uint32_t stash, float& w, int& si, SampleGeo& g)
 {
     const bool valid = k < it.total;
     float f[8];
+    uint32_t pk[3][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i) f[i] = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) pk[m][0] = pk[m][1] = pk[m][2] = pk[m][3] = 0u;
     w = 0.0f;
     si = -1;
     if (valid) {
@@ -475,10 +492,14 @@ __device__ __forceinline__ bool tile_features_half(const FusedParams& p, unsigne
                 gather_half(p, sm, g, m, cb, mat, vec);
 #pragma unroll
                 for (int i = 0; i < 8; ++i) f[i] = m == 2 ? mat[i] * vec[i] : fmaf(mat[i], vec[i], f[i]);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) pk[m][i] = pack_bf16(mat[2 * i], mat[2 * i + 1]);
             }
         }
     }
     store_bf16x8(sm + L.hb[h] + hb_off(t, kH + cb), f);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) tc::st_32x32b_x4(stash + 4 * m, pk[m]);
     return valid;
 }
 
@@ -532,6 +553,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
     tc::fence_after_sync();
     const uint32_t tbase = s_tmem + (uint32_t)(h * 256);
     const uint32_t d0 = tbase, d1 = tbase + 64, dacc = tbase + 128;
+    const uint32_t stash = trow(tbase + 224 + 12 * grp, 0);  // this thread's row, 12 columns
     SegTab tab = seg_tab(reinterpret_cast<float*>(sm + L.segi));
     const float* bias = reinterpret_cast<const float*>(sm + L.bias);
     const float beta = p.mlp.softplus_beta;
@@ -596,7 +618,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             SampleGeo g;
             float w;
             int si;
-            const bool valid = tile_features_half(p, sm, L, tab, it, real, h, t0 + t, t, cb, w, si, g);
+            const bool valid = tile_features_half(p, sm, L, tab, it, real, h, t0 + t, t, cb, stash, w, si, g);
             const float dIw = valid ? tab.acc[si] * w : 0.0f;
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -746,7 +768,11 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             // scratch row, dX * plane values as the line MMA's B operand, and
             // (group 0) the tap column of the line MMA's A operand
             float dx[8];
+            uint32_t pk[3][4];  // BF16 bilinear plane values kept by the feature step
             tc::ld_32x32b_x8(trow(d0, cb), dx);
+            tc::wait_st();
+#pragma unroll
+            for (int m = 0; m < 3; ++m) tc::ld_32x32b_x4(stash + 4 * m, pk[m]);
             tc::wait_ld();
             if (real) {
                 if (grp == 0) {
@@ -756,11 +782,17 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                 }
                 float tsum = 0.f;  // sum of |dX * line value| of this thread's 24 values
                 if (valid) {
-#pragma unroll 1
+#pragma unroll
                     for (int m = 0; m < 3; ++m) {
                         const int Ln = p.field.line_len[m];
                         float mat[8], vec[8], lv[8], gv[8];
-                        gather_half(p, sm, g, m, cb, mat, vec);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const float2 x = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pk[m][i]));
+                            mat[2 * i] = x.x;
+                            mat[2 * i + 1] = x.y;
+                        }
+                        line_half(p, g, m, cb, vec);
 #pragma unroll
                         for (int c = 0; c < 8; ++c) {
                             gv[c] = dx[c] * vec[c];
