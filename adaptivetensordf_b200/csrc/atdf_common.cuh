@@ -96,11 +96,19 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z)
     z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
     return z ^ (z >> 31);
 }
+// The jitter hash in two stages: the ray's key, then the sample's value.
+__device__ __forceinline__ uint64_t jitter_key(uint64_t seed, int32_t ray)
+{
+    return mix64(seed + 0x9e3779b97f4a7c15ULL * (uint64_t)(uint32_t)ray);
+}
+__device__ __forceinline__ float jitter_keyed(uint64_t key, int32_t node, int32_t j)
+{
+    const uint64_t k = mix64(key ^ (((uint64_t)(uint32_t)node << 32) | (uint64_t)(uint32_t)j));
+    return (float)(k >> 40) * (1.0f / 16777216.0f);
+}
 __device__ __forceinline__ float jitter(uint64_t seed, int32_t ray, int32_t node, int32_t j)
 {
-    uint64_t k = mix64(seed + 0x9e3779b97f4a7c15ULL * (uint64_t)(uint32_t)ray);
-    k = mix64(k ^ (((uint64_t)(uint32_t)node << 32) | (uint64_t)(uint32_t)j));
-    return (float)(k >> 40) * (1.0f / 16777216.0f);
+    return jitter_keyed(jitter_key(seed, ray), node, j);
 }
 
 // Interval value a of sample j: explicit array, hash, or the midpoint.

@@ -12,7 +12,7 @@ namespace atdf {
 
 constexpr int kSegItem = 64;          // segments per work item
 constexpr int kLineWin = 64;          // line-gradient window entries per line
-constexpr int kSegTabArrays = 19;     // arrays of the per-item segment table
+constexpr int kSegTabArrays = 27;     // arrays of the per-item segment table
 constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4);  // floats of the per-item table
 
 // ---------------------------------------------------------------------------
@@ -192,6 +192,10 @@ struct SegTab {
     float* size[3];
     float* inv[3];  // 1 / size when size is a power of two, else 0
     int* first;     // global index of the segment's first sample (caller-placed samples)
+    float* org[3];  // the segment's ray: origin and direction
+    float* dir[3];
+    unsigned* key_lo;  // the ray's jitter key (low and high 32 bits)
+    unsigned* key_hi;
 };
 
 __device__ __forceinline__ SegTab seg_tab(float* base)
@@ -214,6 +218,12 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
         t.inv[k] = base + (15 + k) * S;
     }
     t.first = ib + 18 * S;
+    for (int k = 0; k < 3; ++k) {
+        t.org[k] = base + (19 + k) * S;
+        t.dir[k] = base + (22 + k) * S;
+    }
+    t.key_lo = reinterpret_cast<unsigned*>(base + 25 * S);
+    t.key_hi = reinterpret_cast<unsigned*>(base + 26 * S);
     return t;
 }
 
@@ -351,6 +361,15 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
         tab.step[tid] = __fdiv_rn(__fsub_rn(tmax, tmin), (float)n);  // sample_t's step
         tab.acc[tid] = want_dI ? p.grad_image[w.ray[sid]] : 0.0f;
         tab.first[tid] = p.xt ? (int)(w.ray_sample_offset[w.ray[sid]] + w.first[sid]) : 0;
+        const int r = w.ray[sid];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            tab.org[k][tid] = p.origin[3 * r + k];
+            tab.dir[k][tid] = p.dir[3 * r + k];
+        }
+        const uint64_t key = p.seed ? jitter_key(p.seed, r) : 0ull;
+        tab.key_lo[tid] = (unsigned)key;
+        tab.key_hi[tid] = (unsigned)(key >> 32);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
@@ -423,7 +442,6 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
     s.si = find_seg(tab, it.nseg, kk);
     const int j = kk - tab.start[s.si];
     const int n = tab.n[s.si];
-    const int r = tab.ray[s.si];
     s.node = tab.node[s.si];
     const float tmin = tab.tmin[s.si], tmax = tab.tmax[s.si], step = tab.step[s.si];
     float t;
@@ -432,16 +450,18 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
         t = p.xt[gi];
         s.w = p.xw[gi];
     } else {
-        t = sample_t_step(tmin, step, j, sample_a(nullptr, 0, p.seed, r, s.node, j));
-        const float tp =
-            j > 0 ? sample_t_step(tmin, step, j - 1, sample_a(nullptr, 0, p.seed, r, s.node, j - 1)) : 0.0f;
-        const float tn =
-            j < n - 1 ? sample_t_step(tmin, step, j + 1, sample_a(nullptr, 0, p.seed, r, s.node, j + 1)) : 0.0f;
+        // jitter hash of (seed, ray, node, j) from the ray's key in the table
+        // (sample_a's value: the same hash, or 0.5 without a seed)
+        const uint64_t key = ((uint64_t)tab.key_hi[s.si] << 32) | tab.key_lo[s.si];
+        auto a = [&](int jj) { return p.seed ? jitter_keyed(key, s.node, jj) : 0.5f; };
+        t = sample_t_step(tmin, step, j, a(j));
+        const float tp = j > 0 ? sample_t_step(tmin, step, j - 1, a(j - 1)) : 0.0f;
+        const float tn = j < n - 1 ? sample_t_step(tmin, step, j + 1, a(j + 1)) : 0.0f;
         s.w = sample_w(tmin, tmax, n, j, tp, t, tn);
     }
     s.t = t;
 #pragma unroll
-    for (int k2 = 0; k2 < 3; ++k2) s.pos[k2] = __fadd_rn(p.origin[3 * r + k2], __fmul_rn(p.dir[3 * r + k2], t));
+    for (int k2 = 0; k2 < 3; ++k2) s.pos[k2] = __fadd_rn(tab.org[k2][s.si], __fmul_rn(tab.dir[k2][s.si], t));
     return s;
 }
 
