@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kThreads) fused_forward_kernel(FusedParams p)
                 ts = st.t;
                 si = st.si;
                 if (real) {
-                    const SampleGeo g = sample_geo_fast(p, tab, st.si, st.pos);
+                    const SampleGeo g = sample_geo_fast(p, tab, st.node, st.pos);
                     Gathered<CPT> ga;
                     gather_sample<C, CPT>(p, sm, g, q, ga);
                     features_of<C, MODE, CPT>(ga, f);
@@ -524,7 +524,7 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
                 w = st.w;
                 dIw = __fmul_rn(tab.acc[st.si], st.w);
                 if (real) {
-                    g = sample_geo_fast(p, tab, st.si, st.pos);
+                    g = sample_geo_fast(p, tab, st.node, st.pos);
                     Gathered<CPT> ga;
                     gather_sample<C, CPT>(p, sm, g, q, ga);
                     features_of<C, MODE, CPT>(ga, f);

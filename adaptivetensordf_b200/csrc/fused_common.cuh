@@ -10,10 +10,10 @@
 
 namespace atdf {
 
-constexpr int kSegItem = 64;          // segments per work item
+constexpr int kSegItem = 128;         // segments per work item
 constexpr int kLineWin = 64;          // line-gradient window entries per line
-constexpr int kSegTabArrays = 27;     // arrays of the per-item segment table
-constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4);  // floats of the per-item table
+constexpr int kSegTabArrays = 17;     // per-segment arrays of the per-item segment table
+constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4) + 16;  // floats of the table (+ the item's box)
 
 // ---------------------------------------------------------------------------
 // workspace
@@ -177,10 +177,11 @@ struct FusedParams {
 
 constexpr int kBins = ATDF_PROPOSAL_BINS;
 
-// Per-item segment table in shared memory.
+// Per-item segment table in shared memory. The segments of a plane slot's
+// item share one leaf, whose box is kept once (box: min[3], size[3], inverse
+// size[3] when a power of two else 0, then the node id).
 struct SegTab {
     int* start;  // [kSegItem + 1]
-    int* ray;
     int* node;
     int* n;
     int* id;
@@ -188,14 +189,12 @@ struct SegTab {
     float* tmax;
     float* step;  // (tmax - tmin) / n
     float* acc;   // forward partial integral / backward dI of the ray
-    float* bmin[3];
-    float* size[3];
-    float* inv[3];  // 1 / size when size is a power of two, else 0
     int* first;     // global index of the segment's first sample (caller-placed samples)
     float* org[3];  // the segment's ray: origin and direction
     float* dir[3];
     unsigned* key_lo;  // the ray's jitter key (low and high 32 bits)
     unsigned* key_hi;
+    float* box;
 };
 
 __device__ __forceinline__ SegTab seg_tab(float* base)
@@ -204,26 +203,21 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
     SegTab t;
     int* ib = reinterpret_cast<int*>(base);
     t.start = ib;
-    t.ray = ib + S;
-    t.node = ib + 2 * S;
-    t.n = ib + 3 * S;
-    t.id = ib + 4 * S;
-    t.tmin = base + 5 * S;
-    t.tmax = base + 6 * S;
-    t.step = base + 7 * S;
-    t.acc = base + 8 * S;
+    t.node = ib + S;
+    t.n = ib + 2 * S;
+    t.id = ib + 3 * S;
+    t.tmin = base + 4 * S;
+    t.tmax = base + 5 * S;
+    t.step = base + 6 * S;
+    t.acc = base + 7 * S;
+    t.first = ib + 8 * S;
     for (int k = 0; k < 3; ++k) {
-        t.bmin[k] = base + (9 + k) * S;
-        t.size[k] = base + (12 + k) * S;
-        t.inv[k] = base + (15 + k) * S;
+        t.org[k] = base + (9 + k) * S;
+        t.dir[k] = base + (12 + k) * S;
     }
-    t.first = ib + 18 * S;
-    for (int k = 0; k < 3; ++k) {
-        t.org[k] = base + (19 + k) * S;
-        t.dir[k] = base + (22 + k) * S;
-    }
-    t.key_lo = reinterpret_cast<unsigned*>(base + 25 * S);
-    t.key_hi = reinterpret_cast<unsigned*>(base + 26 * S);
+    t.key_lo = reinterpret_cast<unsigned*>(base + 15 * S);
+    t.key_hi = reinterpret_cast<unsigned*>(base + 16 * S);
+    t.box = base + 17 * S;
     return t;
 }
 
@@ -327,8 +321,11 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
         if (s_ctl[4] >= 0 && s_ctl[5] < s_ctl[6]) {
             slot = s_ctl[4];
             const int it = s_ctl[5]++;
-            b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * kSegItem;
-            const int b1 = min(b0 + kSegItem, w.slot_offset[slot + 1]);
+            // the slot's segments in s_ctl[7] items of equal size (<= kSegItem)
+            const int cnt = w.slot_offset[slot + 1] - w.slot_offset[slot];
+            const int per = (cnt + s_ctl[7] - 1) / s_ctl[7];
+            b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * per;
+            const int b1 = min(b0 + per, w.slot_offset[slot + 1]);
             nseg = b1 - b0;
             if (s_ctl[5] == s_ctl[6]) flags |= 2;
         }
@@ -351,7 +348,6 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     if (tid < info.nseg) {
         const int sid = w.bucket[b0 + tid];
         tab.id[tid] = sid;
-        tab.ray[tid] = w.ray[sid];
         tab.node[tid] = w.node[sid];
         tab.n[tid] = w.nsamp[sid];
         const float tmin = w.tmin[sid], tmax = w.tmax[sid];
@@ -370,30 +366,41 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
         const uint64_t key = p.seed ? jitter_key(p.seed, r) : 0ull;
         tab.key_lo[tid] = (unsigned)key;
         tab.key_hi[tid] = (unsigned)(key >> 32);
+        if (tid == 0) {  // the item's leaf (segment 0's; other leaves read the tree)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
-            const float sz = __fsub_rn(mx, mn);
-            tab.bmin[k][tid] = mn;
-            tab.size[k][tid] = sz;
-            tab.inv[k][tid] = pow2_reciprocal(sz);
+            for (int k = 0; k < 3; ++k) {
+                const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
+                const float sz = __fsub_rn(mx, mn);
+                tab.box[k] = mn;
+                tab.box[3 + k] = sz;
+                tab.box[6 + k] = pow2_reciprocal(sz);
+            }
+            reinterpret_cast<int*>(tab.box)[9] = node;
         }
     }
     __syncthreads();
     if (tid < 32) {
-        // exclusive scan of the sample counts (kSegItem = 64: two per lane)
-        const int i0 = 2 * tid, i1 = 2 * tid + 1;
-        const int v0 = i0 < info.nseg ? tab.n[i0] : 0;
-        const int v1 = i1 < info.nseg ? tab.n[i1] : 0;
-        int s = v0 + v1;
+        // exclusive scan of the sample counts (kSegItem = 128: four per lane)
+        constexpr int PL = kSegItem / 32;
+        int v[PL];
+        int s = 0;
+#pragma unroll
+        for (int q = 0; q < PL; ++q) {
+            const int i = PL * tid + q;
+            v[q] = i < info.nseg ? tab.n[i] : 0;
+            s += v[q];
+        }
         int incl = s;
         for (int off = 1; off < 32; off <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, off);
-            if (tid >= off) incl += v;
+            const int x = __shfl_up_sync(0xffffffffu, incl, off);
+            if (tid >= off) incl += x;
         }
-        const int ex = incl - s;
-        tab.start[i0] = ex;
-        tab.start[i1] = ex + v0;
+        int ex = incl - s;
+#pragma unroll
+        for (int q = 0; q < PL; ++q) {
+            tab.start[PL * tid + q] = ex;
+            ex += v[q];
+        }
         if (tid == 31) tab.start[kSegItem] = incl;
     }
     __syncthreads();
@@ -467,12 +474,21 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
 
 // sample_geo with the segment's box from the table and division-free
 // coordinates where the divisor is a power of two (bit-identical).
-__device__ __forceinline__ SampleGeo sample_geo_fast(const FusedParams& p, const SegTab& tab, int si,
+__device__ __forceinline__ SampleGeo sample_geo_fast(const FusedParams& p, const SegTab& tab, int node,
                                                      const float pos[3])
 {
     float loc[3];
+    if (node == reinterpret_cast<const int*>(tab.box)[9]) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) loc[k] = local_coord_fast(pos[k], tab.bmin[k][si], tab.size[k][si], tab.inv[k][si]);
+        for (int k = 0; k < 3; ++k) loc[k] = local_coord_fast(pos[k], tab.box[k], tab.box[3 + k], tab.box[6 + k]);
+    } else {  // a slot shared by several leaves: this sample's box from the tree
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float mn = p.tree.node_position_min[3 * node + k], mx = p.tree.node_position_max[3 * node + k];
+            const float sz = __fsub_rn(mx, mn);
+            loc[k] = local_coord_fast(pos[k], mn, sz, pow2_reciprocal(sz));
+        }
+    }
     SampleGeo g;
     g.pu[0] = loc[1];
     g.pv[0] = loc[2];

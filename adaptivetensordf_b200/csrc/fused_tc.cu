@@ -287,7 +287,7 @@ __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned cha
         ts = st.t;
         si = st.si;
         if (real) {
-            g = sample_geo_fast(p, tab, st.si, st.pos);
+            g = sample_geo_fast(p, tab, st.node, st.pos);
             gather_features(p, sm, g, fa, fb);
         }
     }
@@ -484,7 +484,7 @@ __device__ __forceinline__ bool tile_features_half(const FusedParams& p, unsigne
         w = st.w;
         si = st.si;
         if (real) {
-            g = sample_geo_fast(p, tab, st.si, st.pos);
+            g = sample_geo_fast(p, tab, st.node, st.pos);
             // planes 2, 1, 0, as in gather_features
 #pragma unroll
             for (int m = 2; m >= 0; --m) {
