@@ -7,7 +7,7 @@ The native pieces live next to this file:
   * _atdf_host*.so    the C++/libtorch host layer with the reference's
                       operator surface (HyperTreeBase, SampleList,
                       IndirectGridSample2D/1D, GeometryTensorQO, ...).
-Both are built in place by ``adaptivetensordf_b200.build.build()``. Importing
+Both are built in place by ``adaptivetensordf_b200/build.py``. Importing
 this package loads them and fails loudly when they are missing: there is no
 CPU or pure-PyTorch fallback for the path.
 """
@@ -28,7 +28,7 @@ def _load_ext():
     if not cands or not os.path.exists(LIB_PATH):
         raise ImportError(
             "adaptivetensordf_b200: native libraries are not built; run "
-            "`python -m adaptivetensordf_b200.build` (or __graft_entry__.build())"
+            "`python adaptivetensordf_b200/build.py` (or __graft_entry__.build())"
         )
     from . import _atdf_host  # type: ignore
 
