@@ -13,7 +13,8 @@ namespace atdf {
 constexpr int kSegItem = 128;         // segments per work item
 constexpr int kLineWin = 64;          // line-gradient window entries per line
 constexpr int kSegTabArrays = 17;     // per-segment arrays of the per-item segment table
-constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4) + 16;  // floats of the table (+ the item's box)
+constexpr int kSegMapCap = 4096;      // samples of an item covered by the sample -> segment map
+constexpr int kSegTabFloats = kSegTabArrays * (kSegItem + 4) + 16 + kSegMapCap / 4;  // + the item's box, the map
 
 // ---------------------------------------------------------------------------
 // workspace
@@ -195,6 +196,7 @@ struct SegTab {
     unsigned* key_lo;  // the ray's jitter key (low and high 32 bits)
     unsigned* key_hi;
     float* box;
+    unsigned char* map;  // segment of each sample (items of at most kSegMapCap samples)
 };
 
 __device__ __forceinline__ SegTab seg_tab(float* base)
@@ -218,6 +220,7 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
     t.key_lo = reinterpret_cast<unsigned*>(base + 15 * S);
     t.key_hi = reinterpret_cast<unsigned*>(base + 16 * S);
     t.box = base + 17 * S;
+    t.map = reinterpret_cast<unsigned char*>(t.box + 16);
     return t;
 }
 
@@ -239,6 +242,7 @@ struct ItemInfo {
     bool first;        // first item of its slot: the slot's planes were just requested
     bool last;         // last item of its slot
     int slot_items;    // work items of the slot
+    bool use_map;      // total <= kSegMapCap: the table's map gives each sample's segment
 };
 
 // (k * kSamplePermPrime) mod total without a 64-bit integer division: the
@@ -343,6 +347,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     info.slot_items = s_ctl[7];
     info.total = 0;
     info.inv_total = 0.0;
+    info.use_map = false;
     if (info.slot < 0) return info;
     const int b0 = s_ctl[1];
     if (tid < info.nseg) {
@@ -406,6 +411,14 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     __syncthreads();
     info.total = tab.start[info.nseg];
     info.inv_total = info.total > 0 ? 1.0 / (double)info.total : 0.0;
+    // sample -> segment map (one byte per sample), in place of a binary
+    // search of the count scan per sample
+    info.use_map = info.total <= kSegMapCap;
+    if (info.use_map && tid < info.nseg) {
+        const int b = tab.start[tid], e = tab.start[tid + 1];
+        for (int k = b; k < e; ++k) tab.map[k] = (unsigned char)tid;
+    }
+    __syncthreads();
     return info;
 }
 
@@ -446,7 +459,7 @@ __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const 
 {
     SampleState s;
     const int kk = it.total < kSamplePermPrime ? perm_index(k, it.total, it.inv_total) : k;
-    s.si = find_seg(tab, it.nseg, kk);
+    s.si = it.use_map ? (int)tab.map[kk] : find_seg(tab, it.nseg, kk);
     const int j = kk - tab.start[s.si];
     const int n = tab.n[s.si];
     s.node = tab.node[s.si];

@@ -49,7 +49,7 @@ __device__ __forceinline__ uint32_t w0_off(int n, int f) { return tc::kmajor_off
 __device__ __forceinline__ uint32_t w1_off(int n, int k) { return tc::kmajor_off(n, k, kH); }
 
 struct TCSmem {
-    uint32_t planes, w0, w1, bias, hb[2], g[2], gplanes, gline, sw[2], sdi[2], sseg[2], segi, total;
+    uint32_t planes, w0, w1, bias, hb[2], g[2], gplanes, gline, segi, total;
     __host__ __device__ TCSmem(int plane_elems, int gplane_elems, bool bwd)
     {
         auto al = [](uint32_t x) { return (x + 127u) & ~127u; };
@@ -74,15 +74,6 @@ struct TCSmem {
         if (bwd) o = al(o + gplane_elems * 4);
         gline = o;
         if (bwd) o = al(o + 3 * kLineWinTC * kC * 4);
-        for (int h = 0; h < 2; ++h) {
-            sw[h] = o;
-            o += kRows * 4;
-            sdi[h] = o;
-            o += kRows * 4;
-            sseg[h] = o;
-            o += kRows * 4;
-        }
-        o = al(o);
         segi = o;
         o = al(o + kSegTabFloats * 4);
         total = o;
