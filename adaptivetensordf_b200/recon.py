@@ -354,9 +354,14 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
     tree, geo = build_model(cfg, form, device, init_scale=opt.init_scale, start_depth=opt.start_depth)
 
     def make_optimizer(lr_grid, lr_decoder):
-        a = torch.optim.Adam([{"params": list(geo.planes) + list(geo.lines), "lr": lr_grid},
-                              {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": lr_decoder}],
-                             fused=True)
+        groups = [{"params": list(geo.planes) + list(geo.lines), "lr": lr_grid},
+                  {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": lr_decoder}]
+        if geo.precision == "bf16":  # the step also writes the BF16 working copies
+            from .optim import Adam
+
+            a = Adam(groups, geometry=geo)
+        else:
+            a = torch.optim.Adam(groups, fused=True)
         return a, torch.optim.lr_scheduler.ExponentialLR(a, opt.lr_decay)
 
     adam, sched = make_optimizer(opt.lr_grid, opt.lr_decoder)
@@ -425,8 +430,6 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
                 adam_exp.step()
                 with torch.no_grad():
                     exposure.div_(exposure.mean())
-            if geo.precision == "bf16":
-                geo.RefreshLowPrecision()
             loss_acc += loss.detach().double()
             torch.cuda.synchronize()
             t_train += time.perf_counter() - t0

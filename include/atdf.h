@@ -400,6 +400,19 @@ int atdf_proposal_loss(const atdf_segments_t* segments, const float* features, c
 int atdf_proposal_occupancy(const double* node_mass, const double* node_len, int64_t num_nodes, float* occupancy,
                             atdf_stream_t stream);
 
+/* ---- optimizer step ------------------------------------------------------
+ * Replaces the torch::optim::Adam step the reference builds for the grid and
+ * decoder parameters (geometry_tensor_qo.cpp:79-81, 209-220): torch's Adam
+ * update (no amsgrad; weight_decay is L2 added to the gradient) over n FP32
+ * elements of one parameter, in place on param, exp_avg and exp_avg_sq;
+ * step is the 1-based step count after this update (bias corrections
+ * 1 - beta^step). param_bf16 (nullable) receives the updated parameter
+ * rounded to BF16, the working copy of the BF16 form, in the same pass. All
+ * arrays share one element order (any dense layout, the same for all). */
+int atdf_adam_step(int64_t n, float* param, const float* grad, float* exp_avg, float* exp_avg_sq, void* param_bf16,
+                   float lr, float beta1, float beta2, float eps, float weight_decay, int64_t step,
+                   atdf_stream_t stream);
+
 /* ---- forward projection without device allocation ----------------------
  * No counterpart in the reference (it allocates with torch on every call).
  * For callers that cannot call cudaMalloc (a plugin whose host framework owns

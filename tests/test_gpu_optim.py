@@ -1,0 +1,95 @@
+"""The fused Adam step (atdf_adam_step via adaptivetensordf_b200.optim.Adam)
+against torch.optim.Adam: the same parameters and gradients for several
+steps, with parameter groups, weight decay and a learning-rate change. The
+two evaluate the update in a different operation order, so parameters agree
+to ADAM_RTOL; the BF16 working copies written in the same pass must equal
+the updated FP32 parameters rounded to BF16 exactly."""
+
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+ADAM_RTOL = 1e-5
+ADAM_ATOL = 1e-7
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+
+
+def _pairs(seed):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    shapes = [(37, 16, 17, 17), (1, 16, 256, 1), (64, 16), (1,), (5, 3)]
+    ours, ref = [], []
+    for sh in shapes:
+        x = torch.randn(sh, generator=g)
+        if len(sh) == 4:
+            x = x.contiguous(memory_format=torch.channels_last)
+        a = x.cuda().requires_grad_(True)
+        b = x.clone().cuda().requires_grad_(True)
+        if len(sh) == 4:
+            a = a.detach().contiguous(memory_format=torch.channels_last).requires_grad_(True)
+            b = b.detach().contiguous(memory_format=torch.channels_last).requires_grad_(True)
+        ours.append(a)
+        ref.append(b)
+    return ours, ref
+
+
+def test_fused_adam_matches_torch_adam():
+    from adaptivetensordf_b200 import optim
+
+    ours, ref = _pairs(3)
+    kw = dict(betas=(0.9, 0.99), eps=1e-8)
+    oa = optim.Adam([{"params": ours[:2], "lr": 1e-2}, {"params": ours[2:], "lr": 5e-4, "weight_decay": 0.01}], **kw)
+    ta = torch.optim.Adam([{"params": ref[:2], "lr": 1e-2}, {"params": ref[2:], "lr": 5e-4, "weight_decay": 0.01}],
+                          **kw)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    for step in range(6):
+        for a, b in zip(ours, ref):
+            gr = torch.randn(a.shape, generator=g).cuda()
+            if a.dim() == 4:
+                gr = gr.contiguous(memory_format=torch.channels_last)
+            a.grad = gr.clone()
+            b.grad = gr.clone()
+        if step == 3:  # a schedule step: the new rate is read on the next update
+            for grp_o, grp_t in zip(oa.param_groups, ta.param_groups):
+                grp_o["lr"] *= 0.5
+                grp_t["lr"] *= 0.5
+        oa.step()
+        ta.step()
+    torch.cuda.synchronize()
+    for a, b in zip(ours, ref):
+        torch.testing.assert_close(a.detach(), b.detach(), rtol=ADAM_RTOL, atol=ADAM_ATOL)
+
+
+def test_fused_adam_writes_the_bf16_copies():
+    import adaptivetensordf_b200 as ab  # noqa: F401
+    from adaptivetensordf_b200 import optim
+    from adaptivetensordf_b200 import synthetic as syn
+
+    tree = syn.make_tree(2, device="cuda")
+    geo = syn.make_geometry(tree, 16, 17, (64, 17, 64), [64, 64], seed=9)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    params = syn.parameters(geo)
+    ref = [p.detach().clone() for p in params]
+    opt = optim.Adam(params, lr=1e-2, geometry=geo)
+    tref = torch.optim.Adam([r.requires_grad_(True) for r in ref], lr=1e-2)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    for _ in range(3):
+        for p, r in zip(params, ref):
+            gr = torch.randn(p.shape, generator=g).cuda().contiguous(memory_format=torch.preserve_format)
+            gr = gr.as_strided(p.shape, p.stride()) if gr.stride() != p.stride() else gr
+            p.grad = torch.empty_like(p).copy_(gr)
+            r.grad = torch.empty_like(r).copy_(gr)
+        opt.step()
+        tref.step()
+    torch.cuda.synchronize()
+    for p, r in zip(params, ref):
+        torch.testing.assert_close(p.detach(), r.detach(), rtol=ADAM_RTOL, atol=ADAM_ATOL)
+    for m in range(3):
+        assert torch.equal(geo.planes_bf16[m], geo.planes[m].detach().to(torch.bfloat16))
+        assert torch.equal(geo.lines_bf16[m], geo.lines[m].detach().to(torch.bfloat16))
