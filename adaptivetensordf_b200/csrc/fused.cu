@@ -31,7 +31,18 @@
 namespace atdf {
 
 int launch_ray_segments(const atdf_tree_t& tree, const float* origin, const float* dir, int64_t R, int M,
-                        const atdf_segments_t& segs, int32_t* err, cudaStream_t st);
+                        const atdf_segments_t& segs, int32_t* err, cudaStream_t st, uint32_t* kept_lo = nullptr,
+                        uint32_t* kept_hi = nullptr, int64_t kept_per = 0);
+
+// The workspace's bucket and segment-partial arrays (R * per entries, idle
+// until the segments exist) hold the segment pass's kept hits.
+static int launch_ray_segments_ws(const atdf_tree_t& tree, const float* origin, const float* dir, int64_t R, int M,
+                                  const Ws& w, int32_t* err, cudaStream_t st)
+{
+    const int64_t per = R > 0 ? w.cap / R : 0;
+    return launch_ray_segments(tree, origin, dir, R, M, ws_segments(w), err, st, reinterpret_cast<uint32_t*>(w.bucket),
+                               reinterpret_cast<uint32_t*>(w.seg_partial), per);
+}
 
 constexpr int kThreads = 256;
 constexpr int kT = 32;                // samples per tile
@@ -900,8 +911,8 @@ static int project_forward(const atdf_tree_t* tree, const atdf_field_t* field, c
     p.bins = bins;
     const Ws& w = p.ws;
     if (compute_segments) {
-        st = launch_ray_segments(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, ws_segments(w),
-                                 dev_error, s);
+        st = launch_ray_segments_ws(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, w, dev_error,
+                                    s);
         if (st != ATDF_OK) return st;
     }
     if (bins) ATDF_CUDA_TRY(cudaMemsetAsync(bins, 0, (size_t)w.cap * kBins * sizeof(float), s));
@@ -1014,8 +1025,8 @@ int atdf_project_segments(const atdf_tree_t* tree, const float* ray_origin, cons
     Ws w;
     ws_layout(num_rays, tree->max_depth, num_slots, (char*)workspace, &w);
     *view = ws_segments(w);
-    return launch_ray_segments(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, *view, dev_error,
-                               (cudaStream_t)stream);
+    return launch_ray_segments_ws(*tree, ray_origin, ray_direction, num_rays, max_samples_per_node, w, dev_error,
+                                  (cudaStream_t)stream);
 }
 
 int atdf_project_segment_view(int64_t num_rays, int32_t max_depth, int64_t num_slots, void* workspace,

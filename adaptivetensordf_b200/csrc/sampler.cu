@@ -17,54 +17,94 @@
 
 namespace atdf {
 
-__global__ void scan_exclusive_i64_kernel(int64_t* data, int64_t n, int64_t* total)
+// Exclusive scan of n values with one 1024-thread block: each thread owns a
+// contiguous chunk, loads it 8 values at a time (the loads of a group are in
+// flight together; chunks of up to 16 stay in registers for the write-back),
+// then a warp-shuffle scan of the chunk sums and one of the 32 warp totals.
+template <typename T>
+__device__ __forceinline__ void block_scan_exclusive(T* data, int64_t n, T* total, T* warp_sums)
 {
-    __shared__ int64_t sums[1024];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t per = div_up(n, 1024);
     const int64_t b = min(n, (int64_t)tid * per), e = min(n, b + per);
-    int64_t s = 0;
-    for (int64_t i = b; i < e; ++i) s += data[i];
-    sums[tid] = s;
+    constexpr int KEEP = 16;
+    T keep[KEEP];
+    T s = 0;
+    if (per <= KEEP) {
+#pragma unroll
+        for (int k = 0; k < KEEP; ++k) keep[k] = b + k < e ? data[b + k] : T(0);
+#pragma unroll
+        for (int k = 0; k < KEEP; ++k) s += keep[k];
+    } else {
+        for (int64_t i = b; i < e; i += 8) {
+            T v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = i + k < e ? data[i + k] : T(0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s += v[k];
+        }
+    }
+    T incl = s;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const T x = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += x;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        int64_t v = tid >= off ? sums[tid - off] : 0;
-        __syncthreads();
-        sums[tid] += v;
-        __syncthreads();
+    if (warp == 0) {
+        const T ws = warp_sums[lane];
+        T wi = ws;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const T x = __shfl_up_sync(0xffffffffu, wi, off);
+            if (lane >= off) wi += x;
+        }
+        warp_sums[lane] = wi - ws;  // exclusive warp offsets
+        if (lane == 31 && total) *total = wi;
     }
-    int64_t run = tid ? sums[tid - 1] : 0;
-    for (int64_t i = b; i < e; ++i) {
-        int64_t v = data[i];
-        data[i] = run;
-        run += v;
+    __syncthreads();
+    T run = warp_sums[warp] + incl - s;
+    if (per <= KEEP) {
+#pragma unroll
+        for (int k = 0; k < KEEP; ++k)
+            if (b + k < e) {
+                data[b + k] = run;
+                run += keep[k];
+            }
+    } else {
+        for (int64_t i = b; i < e; i += 8) {
+            T v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = i + k < e ? data[i + k] : T(0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (i + k < e) {
+                    data[i + k] = run;
+                    run += v[k];
+                }
+        }
     }
-    if (tid == 1023 && total) *total = sums[1023];
+    __syncthreads();  // warp_sums is reused by a second scan in the same block
+}
+
+__global__ void scan_exclusive_i64_kernel(int64_t* data, int64_t n, int64_t* total)
+{
+    __shared__ int64_t ws[32];
+    block_scan_exclusive<int64_t>(data, n, total, ws);
+}
+
+// Two arrays of the same length in one launch (blocks 0 and 1).
+__global__ void scan2_exclusive_i64_kernel(int64_t* a, int64_t* b, int64_t n)
+{
+    __shared__ int64_t ws[32];
+    block_scan_exclusive<int64_t>(blockIdx.x == 0 ? a : b, n, nullptr, ws);
 }
 
 __global__ void scan_exclusive_i32_kernel(int32_t* data, int64_t n, int32_t* total)
 {
-    __shared__ int32_t sums[1024];
-    const int tid = threadIdx.x;
-    const int64_t per = div_up(n, 1024);
-    const int64_t b = min(n, (int64_t)tid * per), e = min(n, b + per);
-    int32_t s = 0;
-    for (int64_t i = b; i < e; ++i) s += data[i];
-    sums[tid] = s;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        int32_t v = tid >= off ? sums[tid - off] : 0;
-        __syncthreads();
-        sums[tid] += v;
-        __syncthreads();
-    }
-    int32_t run = tid ? sums[tid - 1] : 0;
-    for (int64_t i = b; i < e; ++i) {
-        int32_t v = data[i];
-        data[i] = run;
-        run += v;
-    }
-    if (tid == 1023 && total) *total = sums[1023];
+    __shared__ int32_t ws[32];
+    block_scan_exclusive<int32_t>(data, n, total, ws);
 }
 
 // bit 0: active leaf; bit 1: some descendant is an active leaf. Bits only
@@ -105,13 +145,23 @@ __global__ void tree_flags_kernel(const int32_t* active, const int32_t* children
 
 constexpr int kSegWarps = 8;
 
-// One warp per ray. WRITE = false: per-ray segment and sample counts.
-// WRITE = true: canonical segments at the scanned offsets.
-template <bool WRITE>
+// Modes of ray_segments_kernel.
+enum SegMode {
+    kSegCount = 0,      // per-ray segment and sample counts
+    kSegWrite = 1,      // traverse again, write the canonical segments at the scanned offsets
+    kSegCountKeep = 2,  // counts, and the ray's sorted hits kept in scratch (kept_per entries per ray)
+    kSegWriteKept = 3,  // write the canonical segments from the kept hits (no traversal)
+};
+
+// One warp per ray.
+template <int MODE>
 __global__ void __launch_bounds__(kSegWarps * 32)
     ray_segments_kernel(atdf_tree_t tree, const float* __restrict__ origin, const float* __restrict__ dir, int64_t R,
-                        int M, atdf_segments_t segs, int32_t* err)
+                        int M, atdf_segments_t segs, int32_t* err, uint32_t* kept_lo, uint32_t* kept_hi,
+                        int64_t kept_per)
 {
+    constexpr bool WRITE = MODE == kSegWrite || MODE == kSegWriteKept;
+    constexpr bool TRAVERSE = MODE != kSegWriteKept;
     __shared__ uint64_t keys[kSegWarps][ATDF_MAX_HITS];
     __shared__ int32_t front[kSegWarps][2][ATDF_MAX_HITS];
     const int lane = threadIdx.x & 31;
@@ -138,6 +188,14 @@ __global__ void __launch_bounds__(kSegWarps * 32)
     int64_t nsamp = 0;
     bool overflow = false;
 
+    if constexpr (!TRAVERSE) {  // the hits kept by the counting pass, already sorted
+        nhit = (int)(segs.ray_seg_offset[r + 1] - segs.ray_seg_offset[r]);
+        const int kmax = (int)(kept_per < ATDF_MAX_HITS ? kept_per : ATDF_MAX_HITS);
+        nhit = max(0, min(nhit, kmax));
+        for (int i = lane; i < nhit; i += 32)
+            key[i] = ((uint64_t)kept_hi[r * kept_per + i] << 32) | kept_lo[r * kept_per + i];
+        __syncwarp();
+    } else {
     // root
     int nfront = 0;
     int cur = 0;
@@ -215,37 +273,52 @@ __global__ void __launch_bounds__(kSegWarps * 32)
 
     // warp total of samples (each lane summed its own hits)
     for (int off = 16; off > 0; off >>= 1) nsamp += __shfl_xor_sync(0xffffffffu, nsamp, off);
+    }
 
-    if (!WRITE) {
+    if constexpr (!WRITE) {
         if (lane == 0) {
             segs.ray_seg_offset[r] = nhit;
             segs.ray_sample_offset[r] = nsamp;
             atomicMax((unsigned long long*)&segs.totals[2], (unsigned long long)nsamp);
             atomicMax((unsigned long long*)&segs.totals[3], (unsigned long long)nhit);
         }
-        return;
+        if constexpr (MODE == kSegCount) return;
     }
 
-    // sort the hits by (tmin, node): bitonic sort of the padded key array
-    int npow = 32;
-    while (npow < nhit) npow <<= 1;
-    for (int i = nhit + lane; i < npow; i += 32) key[i] = ~0ull;
-    __syncwarp();
-    for (int k = 2; k <= npow; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = lane; i < npow; i += 32) {
-                const int ixj = i ^ j;
-                if (ixj > i) {
-                    const uint64_t a = key[i], b = key[ixj];
-                    const bool up = (i & k) == 0;
-                    if ((a > b) == up) {
-                        key[i] = b;
-                        key[ixj] = a;
+    if constexpr (TRAVERSE) {
+        // sort the hits by (tmin, node): bitonic sort of the padded key array
+        int npow = 32;
+        while (npow < nhit) npow <<= 1;
+        for (int i = nhit + lane; i < npow; i += 32) key[i] = ~0ull;
+        __syncwarp();
+        for (int k = 2; k <= npow; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < npow; i += 32) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const uint64_t a = key[i], b = key[ixj];
+                        const bool up = (i & k) == 0;
+                        if ((a > b) == up) {
+                            key[i] = b;
+                            key[ixj] = a;
+                        }
                     }
                 }
+                __syncwarp();
             }
-            __syncwarp();
         }
+    }
+
+    if constexpr (MODE == kSegCountKeep) {  // keep the sorted hits for the writing pass
+        if (nhit > kept_per) {
+            if (lane == 0) set_err(err, ATDF_DEVERR_SEG_CAPACITY);
+            return;
+        }
+        for (int i = lane; i < nhit; i += 32) {
+            kept_lo[r * kept_per + i] = (uint32_t)key[i];
+            kept_hi[r * kept_per + i] = (uint32_t)(key[i] >> 32);
+        }
+        return;
     }
 
     const int64_t seg0 = segs.ray_seg_offset[r];
@@ -262,7 +335,11 @@ __global__ void __launch_bounds__(kSegWarps * 32)
         const int i = lane * PER + q;
         nloc[q] = 0;
         if (i < nhit) {
-            const int node = (int)(key[i] & 0xffffffffu);
+            int node = (int)(key[i] & 0xffffffffu);
+            if (node < 0 || node >= tree.num_nodes) {  // kept hits of a ray that overflowed its slots
+                set_err(err, ATDF_DEVERR_INDEX);
+                node = 0;
+            }
             float tmin, tmax;
             intersect_box(pmin + 3 * (int64_t)node, pmax + 3 * (int64_t)node, o, d, tmin, tmax);
             nloc[q] = seg_num_samples(pmin + 3 * (int64_t)node, pmax + 3 * (int64_t)node, tmin, tmax, M);
@@ -395,29 +472,41 @@ __global__ void node_id_kernel(atdf_tree_t tree, const int64_t* __restrict__ act
     }
 }
 
-// Launch helpers shared with the fused path.
+// Launch helpers shared with the fused path. kept_lo / kept_hi (nullable):
+// scratch of R * kept_per entries each where the counting pass keeps every
+// ray's sorted hits, so that the writing pass does not traverse the tree again.
 int launch_ray_segments(const atdf_tree_t& tree, const float* origin, const float* dir, int64_t R, int M,
-                        const atdf_segments_t& segs, int32_t* err, cudaStream_t st)
+                        const atdf_segments_t& segs, int32_t* err, cudaStream_t st, uint32_t* kept_lo = nullptr,
+                        uint32_t* kept_hi = nullptr, int64_t kept_per = 0)
 {
     ATDF_CUDA_TRY(cudaMemsetAsync(segs.totals, 0, 4 * sizeof(int64_t), st));
     const int64_t blocks = div_up(R, kSegWarps);
+    const bool keep = kept_lo && kept_hi && kept_per > 0;
     if (R > 0) {
-        ray_segments_kernel<false><<<(unsigned)blocks, kSegWarps * 32, 0, st>>>(tree, origin, dir, R, M, segs, err);
+        if (keep)
+            ray_segments_kernel<kSegCountKeep><<<(unsigned)blocks, kSegWarps * 32, 0, st>>>(
+                tree, origin, dir, R, M, segs, err, kept_lo, kept_hi, kept_per);
+        else
+            ray_segments_kernel<kSegCount><<<(unsigned)blocks, kSegWarps * 32, 0, st>>>(tree, origin, dir, R, M, segs,
+                                                                                       err, nullptr, nullptr, 0);
         ATDF_LAUNCH_CHECK();
     } else {
         ATDF_CUDA_TRY(cudaMemsetAsync(segs.ray_seg_offset, 0, sizeof(int64_t), st));
         ATDF_CUDA_TRY(cudaMemsetAsync(segs.ray_sample_offset, 0, sizeof(int64_t), st));
     }
-    scan_exclusive_i64_kernel<<<1, 1024, 0, st>>>(segs.ray_seg_offset, R + 1, nullptr);
-    ATDF_LAUNCH_CHECK();
-    scan_exclusive_i64_kernel<<<1, 1024, 0, st>>>(segs.ray_sample_offset, R + 1, nullptr);
+    scan2_exclusive_i64_kernel<<<2, 1024, 0, st>>>(segs.ray_seg_offset, segs.ray_sample_offset, R + 1);
     ATDF_LAUNCH_CHECK();
     ATDF_CUDA_TRY(cudaMemcpyAsync(&segs.totals[0], &segs.ray_seg_offset[R], sizeof(int64_t),
                                   cudaMemcpyDeviceToDevice, st));
     ATDF_CUDA_TRY(cudaMemcpyAsync(&segs.totals[1], &segs.ray_sample_offset[R], sizeof(int64_t),
                                   cudaMemcpyDeviceToDevice, st));
     if (R > 0) {
-        ray_segments_kernel<true><<<(unsigned)blocks, kSegWarps * 32, 0, st>>>(tree, origin, dir, R, M, segs, err);
+        if (keep)
+            ray_segments_kernel<kSegWriteKept><<<(unsigned)blocks, kSegWarps * 32, 0, st>>>(
+                tree, origin, dir, R, M, segs, err, kept_lo, kept_hi, kept_per);
+        else
+            ray_segments_kernel<kSegWrite><<<(unsigned)blocks, kSegWarps * 32, 0, st>>>(tree, origin, dir, R, M, segs,
+                                                                                       err, nullptr, nullptr, 0);
         ATDF_LAUNCH_CHECK();
     }
     return ATDF_OK;
