@@ -502,8 +502,7 @@ __global__ void __launch_bounds__(kThreads, 1) fused_backward_kernel(FusedParams
                 *reinterpret_cast<float4*>(sm + L.gplanes + i) = make_float4(0.f, 0.f, 0.f, 0.f);
             for (int i = tid; i < 3 * kLineWin * C; i += kThreads) sm[L.gline + i] = 0.0f;
             if (tid < 3) {
-                float bmin[3], bmax[3];
-                item_box(p, tab.node[0], bmin, bmax);
+                const float* bmin = tab.box;  // the item's leaf (segment 0's)
                 const int Ln = p.field.line_len[tid];
                 int lo = 0;
                 if (Ln > kLineWin) {

@@ -280,6 +280,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
 {
     const Ws& w = p.ws;
     const int tid = threadIdx.x;
+    if (tid < 32) {
     if (tid == 0) {
         int slot = -1, b0 = 0, nseg = 0, flags = 0;
         if (s_ctl[5] >= s_ctl[6]) {  // the current slot is done: take the next one with work
@@ -299,27 +300,13 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
                 }
             }
             if (s_ctl[4] >= 0 && s_ctl[4] < w.nslot) {
-                const int64_t sl = s_ctl[4];
                 // plane_off counts elements of the plane type (4 or 2 bytes)
                 const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
                 uint32_t bytes = 0;
                 for (int m = 0; m < 3; ++m)
                     bytes += (uint32_t)(p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels * esz);
-                fence_proxy_async();
                 mbar_expect_tx(bar, bytes);
-                for (int m = 0; m < 3; ++m) {
-                    const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
-                    char* dst = reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz;
-                    const char* src = reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz;
-                    if (p.plane_pitch[m] == p.field.plane_w[m]) {
-                        tma_bulk_load(dst, src, (uint32_t)(pf * esz), bar);
-                    } else {  // padded rows: one copy per row
-                        const uint32_t row = (uint32_t)(p.field.plane_w[m] * p.field.channels * esz);
-                        const uint32_t pitch = (uint32_t)(p.plane_pitch[m] * p.field.channels * esz);
-                        for (int r = 0; r < p.field.plane_h[m]; ++r)
-                            tma_bulk_load(dst + (size_t)r * pitch, src + (size_t)r * row, row, bar);
-                    }
-                }
+                flags |= 4;  // warp 0 issues the slot's plane copies below
             }
         }
         if (s_ctl[4] >= 0 && s_ctl[5] < s_ctl[6]) {
@@ -337,6 +324,31 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
         s_ctl[1] = b0;
         s_ctl[2] = nseg;
         s_ctl[3] = flags;
+    }
+    __syncwarp();
+    if (s_ctl[3] & 4) {  // a new plane slot: its three planes, the copies spread over warp 0's lanes
+        const int64_t sl = s_ctl[4];
+        const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
+        fence_proxy_async();
+        // copy c of plane m: its whole plane (unpadded) or its row c (padded)
+        int c0 = 0;
+        for (int m = 0; m < 3; ++m) {
+            const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
+            char* dst = reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz;
+            const char* src = reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz;
+            const bool padded = p.plane_pitch[m] != p.field.plane_w[m];
+            const int ncopy = padded ? p.field.plane_h[m] : 1;
+            const uint32_t row = (uint32_t)(p.field.plane_w[m] * p.field.channels * esz);
+            const uint32_t pitch = (uint32_t)(p.plane_pitch[m] * p.field.channels * esz);
+            for (int c = ((tid - c0) % 32 + 32) % 32; c < ncopy; c += 32) {
+                if (padded)
+                    tma_bulk_load(dst + (size_t)c * pitch, src + (size_t)c * row, row, bar);
+                else
+                    tma_bulk_load(dst, src, (uint32_t)(pf * esz), bar);
+            }
+            c0 += ncopy;
+        }
+    }
     }
     __syncthreads();
     ItemInfo info;
@@ -527,16 +539,6 @@ __device__ __forceinline__ void add_to_bins(const FusedParams& p, const SegTab& 
     b = b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
     atomicAdd(&p.bins[(int64_t)tab.id[si] * kBins + b], v);
 }
-
-__device__ __forceinline__ void item_box(const FusedParams& p, int node, float* bmin, float* bmax)
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        bmin[k] = p.tree.node_position_min[3 * node + k];
-        bmax[k] = p.tree.node_position_max[3 * node + k];
-    }
-}
-
 
 // BF16 tensor-core variant (fused_tc.cu).
 bool tc_supported(const atdf_field_t* f, const atdf_mlp_t* m);

@@ -578,8 +578,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             ntiles = 0;
             for (int i = tid; i < 3 * kLineWinTC * C; i += kThreadsB2) gln[i] = 0.0f;
             if (tid < 3) {
-                float bmin[3], bmax[3];
-                item_box(p, tab.node[0], bmin, bmax);
+                const float* bmin = tab.box;  // the item's leaf (segment 0's)
                 const int Ln = p.field.line_len[tid];
                 int lo = 0;
                 if (Ln > kLineRowsTC) {
