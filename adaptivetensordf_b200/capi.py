@@ -156,6 +156,7 @@ def _declare(L):
         "atdf_proposal_loss": (I32, [ct.POINTER(Segments), P, P, P, F32, P, P, P, P, I64, P, P]),
         "atdf_proposal_occupancy": (I32, [P, P, I64, P, P]),
         "atdf_adam_step": (I32, [I64, P, P, P, P, P, F32, F32, F32, F32, F32, I64, P]),
+        "atdf_camera_rays": (I32, [I64, P, P, P, P, P, I64, P, I64, I32, I32, I32, I32, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -390,7 +390,7 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
 
     def evaluate(epoch):
         nonlocal reached
-        p = psnr(tree, geo, data.volume)
+        p = psnr(tree, geo, data.volume) if data.volume is not None else None  # no ground truth: loss only
         rec = {"form": form, "t": t_train, "step": step, "epoch": epoch, "psnr": p,
                "loss": float(loss_acc) / max(1, step)}
         if prop is not None:
@@ -398,7 +398,7 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         records.append(rec)
         if log:
             log(rec)
-        if reached is None and p >= opt.target_psnr:
+        if reached is None and p is not None and p >= opt.target_psnr:
             reached = t_train
         return p
 
@@ -482,12 +482,19 @@ def main():
     ap.add_argument("--refine-every", type=int, default=0)
     ap.add_argument("--max-leaves", type=int, default=0)
     ap.add_argument("--tone-mapper", action="store_true")
+    ap.add_argument("--scene", default="", help="train on a scene directory (dataset.ini, camera.ini, poses.txt, "
+                                                 "images.txt, numpy projections) instead of the synthetic series")
     a = ap.parse_args()
     cfg = syn.CONFIGS[a.config]
     if a.noise >= 0:
         cfg = dataclasses.replace(cfg, noise=a.noise, jitter=0.0 if a.noise == 0 else cfg.jitter)
     t0 = time.perf_counter()
-    data = make_tilt_series(cfg)
+    if a.scene:
+        from .scene import load_scene
+
+        data = load_scene(a.scene).tilt_series()
+    else:
+        data = make_tilt_series(cfg)
     torch.cuda.synchronize()
     print(json.dumps({"data_s": time.perf_counter() - t0, "rays": data.num_rays}), flush=True)
     opt = TrainOptions(epochs=a.epochs, batch=a.batch or cfg.rays_per_batch,

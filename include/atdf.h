@@ -400,6 +400,25 @@ int atdf_proposal_loss(const atdf_segments_t* segments, const float* features, c
 int atdf_proposal_occupancy(const double* node_mass, const double* node_len, int64_t num_nodes, float* occupancy,
                             atdf_stream_t stream);
 
+/* ---- rays of detector pixels ---------------------------------------------
+ * SceneBase::GetRays (SceneBase.cpp:369-450) with UVToPixel
+ * (CameraPose.h:14-30) and CameraModelModule::Unproject (CameraPose.cu:469-479)
+ * for n pixels: uv [n,2] in [0,1] (pixel centres at (i + 0.5) / w without
+ * align_corners), image_id [n], camera_id [n] (nullable: camera 0); per image
+ * rotation [num_images,4] unit quaternions (x, y, z, w) and translation
+ * [num_images,3] (pinhole only, nullable otherwise); per camera intrinsics
+ * [num_cameras,5] = fx fy cx cy s; volume_translation: host float[3]
+ * (orthographic only, nullable = 0). FP64 arithmetic, FP32 outputs
+ * origin / direction [n,3]. An out-of-range image or camera index sets
+ * ATDF_DEVERR_INDEX and leaves that ray unwritten. */
+#define ATDF_CAMERA_PINHOLE 0
+#define ATDF_CAMERA_ORTHOGRAPHIC 1
+int atdf_camera_rays(int64_t n, const float* uv, const int32_t* image_id, const int32_t* camera_id,
+                     const double* rotation, const double* translation, int64_t num_images, const double* intrinsics,
+                     int64_t num_cameras, int32_t width, int32_t height, int32_t align_corners, int32_t model,
+                     const float* volume_translation, float* origin, float* direction, int32_t* dev_error,
+                     atdf_stream_t stream);
+
 /* ---- optimizer step ------------------------------------------------------
  * Replaces the torch::optim::Adam step the reference builds for the grid and
  * decoder parameters (geometry_tensor_qo.cpp:79-81, 209-220): torch's Adam
