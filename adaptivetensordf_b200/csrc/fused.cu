@@ -80,6 +80,20 @@ __global__ void item_count_kernel(Ws w)
     }
 }
 
+// Zeroes the plane gradients of the slots that no segment touches; the
+// tensor-core backward writes every touched slot's gradient itself.
+__global__ void zero_untouched_slots_kernel(Ws w, atdf_field_grad_t g, atdf_field_t f)
+{
+    for (int64_t s = blockIdx.x; s < w.nslot; s += gridDim.x) {
+        if (w.item_offset[s + 1] > w.item_offset[s]) continue;
+        for (int m = 0; m < 3; ++m) {
+            const int64_t pf = (int64_t)f.plane_h[m] * f.plane_w[m] * f.channels;
+            float* dst = g.plane[m] + s * pf;
+            for (int64_t i = threadIdx.x; i < pf; i += blockDim.x) dst[i] = 0.0f;
+        }
+    }
+}
+
 // Per-ray sum of the segment partials, in segment (t) order.
 __global__ void ray_reduce_kernel(Ws w, int64_t R, float* image)
 {
@@ -962,10 +976,19 @@ static int project_backward(const atdf_tree_t* tree, const atdf_field_t* field, 
     p.xt = xt;
     p.xw = xw;
     for (int m = 0; m < 3; ++m) {
-        const size_t pf = (size_t)field->plane_h[m] * field->plane_w[m] * field->channels * field->num_slots;
-        ATDF_CUDA_TRY(cudaMemsetAsync(grad_field->plane[m], 0, pf * 4, s));
+        // the tensor-core backward writes the plane gradient of every slot
+        // it touches (zeroing it first) and the rest is zeroed below
+        if (var) {
+            const size_t pf = (size_t)field->plane_h[m] * field->plane_w[m] * field->channels * field->num_slots;
+            ATDF_CUDA_TRY(cudaMemsetAsync(grad_field->plane[m], 0, pf * 4, s));
+        }
         ATDF_CUDA_TRY(
             cudaMemsetAsync(grad_field->line[m], 0, (size_t)field->line_len[m] * field->channels * 4, s));
+    }
+    if (!var && p.ws.nslot > 0) {
+        zero_untouched_slots_kernel<<<(unsigned)std::min<int64_t>(p.ws.nslot, 592), 256, 0, s>>>(p.ws, *grad_field,
+                                                                                                *field);
+        ATDF_LAUNCH_CHECK();
     }
     for (int l = 0; l < mlp->num_layers; ++l) {
         ATDF_CUDA_TRY(cudaMemsetAsync(grad_mlp->weight[l], 0, (size_t)mlp->dims[l] * mlp->dims[l + 1] * 4, s));

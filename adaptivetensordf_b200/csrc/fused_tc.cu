@@ -568,6 +568,14 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
         if (real && it.first) {
             for (int i = tid * 4; i < gplane_elems; i += kThreadsB2 * 4)
                 *reinterpret_cast<int4*>(gpl + i) = make_int4(0, 0, 0, 0);
+            // the slot's global gradient starts at zero (the caller does not
+            // clear it): a tile that overflows the fixed-point range adds to it
+            for (int m = 0; m < 3; ++m) {
+                const int pf = p.field.plane_h[m] * p.field.plane_w[m] * C;
+                float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
+                for (int i = tid * 4; i < pf; i += kThreadsB2 * 4)
+                    *reinterpret_cast<float4*>(dst + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             if (tid == 0) {
                 s_tcum[0] = s_tcum[1] = 0.f;
                 s_tfirst[0] = s_tfirst[1] = 0.f;
