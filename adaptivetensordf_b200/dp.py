@@ -26,14 +26,31 @@ def shard_permutation(num_rays: int, batch: int, rank: int, world: int, epoch: i
     return [perm[s * per_step + rank * batch: s * per_step + (rank + 1) * batch] for s in range(steps)]
 
 
-def allreduce_gradients(params, world: int):
-    """Average the .grad of every parameter over the ranks (in place)."""
+def allreduce_gradients(params, world: int, bucket_bytes: int = 1 << 20):
+    """Average the .grad of every parameter over the ranks (in place). Each
+    gradient of at least bucket_bytes is reduced on its own; the smaller ones
+    (decoder weights and biases, lines) travel together in one flat buffer per
+    dtype, one collective instead of one each (their cost is latency, not
+    bandwidth). Every rank issues the same collectives in the same order."""
     if world <= 1:
         return
-    for p in params:
-        if p.grad is not None:
-            dist.all_reduce(p.grad, op=dist.ReduceOp.SUM)
-            p.grad.div_(world)
+    grads = [p.grad for p in params if p.grad is not None]
+    small = {}
+    for g in grads:
+        if g.numel() * g.element_size() >= bucket_bytes:
+            dist.all_reduce(g, op=dist.ReduceOp.SUM)
+            g.div_(world)
+        else:
+            small.setdefault((g.dtype, g.device), []).append(g)
+    for group in small.values():
+        flat = torch.cat([g.reshape(-1) for g in group])
+        dist.all_reduce(flat, op=dist.ReduceOp.SUM)
+        flat.div_(world)
+        off = 0
+        for g in group:
+            n = g.numel()
+            g.copy_(flat[off:off + n].view(g.shape))
+            off += n
 
 
 def allreduce_node_error(loss_sum: torch.Tensor, weight_sum: torch.Tensor, world: int):

@@ -30,12 +30,17 @@ def _worker(rank, world, port, out):
         p.grad = torch.full((5,), float(rank + 1))
         q = torch.nn.Parameter(torch.zeros(2, 2))
         q.grad = torch.eye(2) * (rank + 1) * 10
-        dp.allreduce_gradients([p, q], world)
+        # a gradient above the bucket size (reduced alone, channels-last like
+        # the planes) and two below it (reduced together in one flat buffer)
+        big = torch.nn.Parameter(torch.zeros(2, 3, 4, 5).contiguous(memory_format=torch.channels_last))
+        big.grad = (torch.arange(120.0).reshape(2, 3, 4, 5) * (rank + 1)).contiguous(
+            memory_format=torch.channels_last)
+        dp.allreduce_gradients([p, big, q], world, bucket_bytes=64)
         ls = torch.arange(4, dtype=torch.float64) * (rank + 1)
         ws = torch.ones(4, dtype=torch.float64)
         dp.allreduce_node_error(ls, ws, world)
         out[rank] = {"shards": [s.tolist() for s in shards], "p": p.grad.tolist(), "q": q.grad.tolist(),
-                     "ls": ls.tolist(), "ws": ws.tolist()}
+                     "big": big.grad.tolist(), "ls": ls.tolist(), "ws": ws.tolist()}
     finally:
         dist.destroy_process_group()
 
@@ -54,4 +59,5 @@ def test_two_rank_data_parallel_step():
     for r in (a, b):
         assert r["p"] == [1.5] * 5
         assert r["q"] == [[15.0, 0.0], [0.0, 15.0]]
+        assert r["big"] == (torch.arange(120.0).reshape(2, 3, 4, 5) * 1.5).tolist()
         assert r["ls"] == [0.0, 3.0, 6.0, 9.0] and r["ws"] == [2.0] * 4
