@@ -659,13 +659,26 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
 #pragma unroll
                 for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bb[i];
             }
+            // one logistic per element: a1 becomes silu(A1), gpk keeps
+            // silu'(A1) (in [-0.1, 1.1]) as packed FP16 for dA1
             float zp = 0.f;
+            __half2 gpk[16];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 float ww[16];
                 ld16(bias + 2 * kH + col0 + 16 * j, ww);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) zp = fmaf(silu(a1[16 * j + i]), ww[i], zp);
+                for (int i = 0; i < 16; i += 2) {
+                    const float x0 = a1[16 * j + i], x1 = a1[16 * j + i + 1];
+                    const float s0 = sigmoid_tanh(x0), s1 = sigmoid_tanh(x1);
+                    const float h0 = x0 * s0, h1 = x1 * s1;
+                    gpk[(16 * j + i) >> 1] = __floats2half2_rn(s0 * (1.0f + x0 * (1.0f - s0)),
+                                                               s1 * (1.0f + x1 * (1.0f - s1)));
+                    a1[16 * j + i] = h0;
+                    a1[16 * j + i + 1] = h1;
+                    zp = fmaf(h0, ww[i], zp);
+                    zp = fmaf(h1, ww[i + 1], zp);
+                }
             }
             s_z[h][grp][t] = zp;
             half_barrier2(h);
@@ -677,7 +690,11 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                 float ww[16], da[16];
                 ld16(bias + 2 * kH + col0 + 16 * j, ww);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) da[i] = dz * ww[i] * silu_grad(a1[16 * j + i]);
+                for (int i = 0; i < 16; i += 2) {
+                    const float2 g = __half22float2(gpk[(16 * j + i) >> 1]);
+                    da[i] = dz * ww[i] * g.x;
+                    da[i + 1] = dz * ww[i + 1] * g.y;
+                }
                 store_bf16x8(gh + g_off(t, col0 + 16 * j), da);
                 store_bf16x8(gh + g_off(t, col0 + 16 * j + 8), da + 8);
             }
@@ -686,7 +703,7 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
             // with one column
             {
 #pragma unroll
-                for (int k = 0; k < 32; ++k) a1[k] = dz * silu(a1[k]);
+                for (int k = 0; k < 32; ++k) a1[k] = dz * a1[k];
                 int n = 32;
 #pragma unroll
                 for (int off = 16; off >= 1; off >>= 1) {
