@@ -470,10 +470,13 @@ def main():
     ap.add_argument("--time-limit", type=float, default=0.0)
     ap.add_argument("--lr-grid", type=float, default=0.01)
     ap.add_argument("--lr-decoder", type=float, default=5e-4)
+    ap.add_argument("--lr-decay", type=float, default=0.95, help="learning-rate factor per epoch")
     ap.add_argument("--no-stop", action="store_true")
     ap.add_argument("--tv", type=float, default=0.0)
     ap.add_argument("--init-scale", type=float, default=0.5)
     ap.add_argument("--noise", type=float, default=-1.0, help="override the config's noise level")
+    ap.add_argument("--angles", type=int, default=0, help="override the number of tilts")
+    ap.add_argument("--angle-step", type=float, default=0.0, help="override the tilt step (degrees)")
     ap.add_argument("--budget", type=int, default=64)
     ap.add_argument("--gate", type=float, default=0.01)
     ap.add_argument("--judge-every", type=int, default=10)
@@ -488,6 +491,10 @@ def main():
     cfg = syn.CONFIGS[a.config]
     if a.noise >= 0:
         cfg = dataclasses.replace(cfg, noise=a.noise, jitter=0.0 if a.noise == 0 else cfg.jitter)
+    if a.angles:
+        cfg = dataclasses.replace(cfg, angles=a.angles)
+    if a.angle_step:
+        cfg = dataclasses.replace(cfg, angle_step=a.angle_step)
     t0 = time.perf_counter()
     if a.scene:
         from .scene import load_scene
@@ -500,7 +507,8 @@ def main():
     opt = TrainOptions(epochs=a.epochs, batch=a.batch or cfg.rays_per_batch,
                        max_samples_per_node=a.samples or cfg.max_samples_per_node, eval_every=a.eval_every,
                        target_psnr=a.target, time_limit=a.time_limit, stop_at_target=not a.no_stop,
-                       lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, loss_tv=a.tv, init_scale=a.init_scale,
+                       lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, lr_decay=a.lr_decay, loss_tv=a.tv,
+                       init_scale=a.init_scale,
                        budget=a.budget, gate=a.gate, judge_every=a.judge_every,
                        proposal_jitter=not a.no_prop_jitter, start_depth=a.start_depth,
                        refine_every=a.refine_every, max_active_nodes=a.max_leaves, tone_mapper=a.tone_mapper)
