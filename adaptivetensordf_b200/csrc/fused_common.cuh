@@ -281,74 +281,74 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     const Ws& w = p.ws;
     const int tid = threadIdx.x;
     if (tid < 32) {
-    if (tid == 0) {
-        int slot = -1, b0 = 0, nseg = 0, flags = 0;
-        if (s_ctl[5] >= s_ctl[6]) {  // the current slot is done: take the next one with work
-            const int nslots = (int)w.nslot + 1;  // plane slots + the out-of-ROI bucket
-            s_ctl[4] = -1;
-            while (true) {
-                const int sl = atomicAdd(&w.counters[queue], 1);
-                if (sl >= nslots) break;
-                const int i0 = w.item_offset[sl], i1 = w.item_offset[sl + 1];
-                if (i1 > i0) {
-                    s_ctl[4] = sl;
-                    s_ctl[5] = i0;
-                    s_ctl[6] = i1;
-                    s_ctl[7] = i1 - i0;
-                    flags |= 1;
-                    break;
+        if (tid == 0) {
+            int slot = -1, b0 = 0, nseg = 0, flags = 0;
+            if (s_ctl[5] >= s_ctl[6]) {  // the current slot is done: take the next one with work
+                const int nslots = (int)w.nslot + 1;  // plane slots + the out-of-ROI bucket
+                s_ctl[4] = -1;
+                while (true) {
+                    const int sl = atomicAdd(&w.counters[queue], 1);
+                    if (sl >= nslots) break;
+                    const int i0 = w.item_offset[sl], i1 = w.item_offset[sl + 1];
+                    if (i1 > i0) {
+                        s_ctl[4] = sl;
+                        s_ctl[5] = i0;
+                        s_ctl[6] = i1;
+                        s_ctl[7] = i1 - i0;
+                        flags |= 1;
+                        break;
+                    }
+                }
+                if (s_ctl[4] >= 0 && s_ctl[4] < w.nslot) {
+                    // plane_off counts elements of the plane type (4 or 2 bytes)
+                    const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
+                    uint32_t bytes = 0;
+                    for (int m = 0; m < 3; ++m)
+                        bytes += (uint32_t)(p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels * esz);
+                    mbar_expect_tx(bar, bytes);
+                    flags |= 4;  // warp 0 issues the slot's plane copies below
                 }
             }
-            if (s_ctl[4] >= 0 && s_ctl[4] < w.nslot) {
-                // plane_off counts elements of the plane type (4 or 2 bytes)
-                const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
-                uint32_t bytes = 0;
-                for (int m = 0; m < 3; ++m)
-                    bytes += (uint32_t)(p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels * esz);
-                mbar_expect_tx(bar, bytes);
-                flags |= 4;  // warp 0 issues the slot's plane copies below
+            if (s_ctl[4] >= 0 && s_ctl[5] < s_ctl[6]) {
+                slot = s_ctl[4];
+                const int it = s_ctl[5]++;
+                // the slot's segments in s_ctl[7] items of equal size (<= kSegItem)
+                const int cnt = w.slot_offset[slot + 1] - w.slot_offset[slot];
+                const int per = (cnt + s_ctl[7] - 1) / s_ctl[7];
+                b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * per;
+                const int b1 = min(b0 + per, w.slot_offset[slot + 1]);
+                nseg = b1 - b0;
+                if (s_ctl[5] == s_ctl[6]) flags |= 2;
+            }
+            s_ctl[0] = slot;
+            s_ctl[1] = b0;
+            s_ctl[2] = nseg;
+            s_ctl[3] = flags;
+        }
+        __syncwarp();
+        if (s_ctl[3] & 4) {  // a new plane slot: its three planes, the copies spread over warp 0's lanes
+            const int64_t sl = s_ctl[4];
+            const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
+            fence_proxy_async();
+            // copy c of plane m: its whole plane (unpadded) or its row c (padded)
+            int c0 = 0;
+            for (int m = 0; m < 3; ++m) {
+                const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
+                char* dst = reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz;
+                const char* src = reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz;
+                const bool padded = p.plane_pitch[m] != p.field.plane_w[m];
+                const int ncopy = padded ? p.field.plane_h[m] : 1;
+                const uint32_t row = (uint32_t)(p.field.plane_w[m] * p.field.channels * esz);
+                const uint32_t pitch = (uint32_t)(p.plane_pitch[m] * p.field.channels * esz);
+                for (int c = ((tid - c0) % 32 + 32) % 32; c < ncopy; c += 32) {
+                    if (padded)
+                        tma_bulk_load(dst + (size_t)c * pitch, src + (size_t)c * row, row, bar);
+                    else
+                        tma_bulk_load(dst, src, (uint32_t)(pf * esz), bar);
+                }
+                c0 += ncopy;
             }
         }
-        if (s_ctl[4] >= 0 && s_ctl[5] < s_ctl[6]) {
-            slot = s_ctl[4];
-            const int it = s_ctl[5]++;
-            // the slot's segments in s_ctl[7] items of equal size (<= kSegItem)
-            const int cnt = w.slot_offset[slot + 1] - w.slot_offset[slot];
-            const int per = (cnt + s_ctl[7] - 1) / s_ctl[7];
-            b0 = w.slot_offset[slot] + (it - w.item_offset[slot]) * per;
-            const int b1 = min(b0 + per, w.slot_offset[slot + 1]);
-            nseg = b1 - b0;
-            if (s_ctl[5] == s_ctl[6]) flags |= 2;
-        }
-        s_ctl[0] = slot;
-        s_ctl[1] = b0;
-        s_ctl[2] = nseg;
-        s_ctl[3] = flags;
-    }
-    __syncwarp();
-    if (s_ctl[3] & 4) {  // a new plane slot: its three planes, the copies spread over warp 0's lanes
-        const int64_t sl = s_ctl[4];
-        const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
-        fence_proxy_async();
-        // copy c of plane m: its whole plane (unpadded) or its row c (padded)
-        int c0 = 0;
-        for (int m = 0; m < 3; ++m) {
-            const int64_t pf = (int64_t)p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels;
-            char* dst = reinterpret_cast<char*>(sm) + (size_t)p.plane_off[m] * esz;
-            const char* src = reinterpret_cast<const char*>(p.field.plane[m]) + (size_t)sl * pf * esz;
-            const bool padded = p.plane_pitch[m] != p.field.plane_w[m];
-            const int ncopy = padded ? p.field.plane_h[m] : 1;
-            const uint32_t row = (uint32_t)(p.field.plane_w[m] * p.field.channels * esz);
-            const uint32_t pitch = (uint32_t)(p.plane_pitch[m] * p.field.channels * esz);
-            for (int c = ((tid - c0) % 32 + 32) % 32; c < ncopy; c += 32) {
-                if (padded)
-                    tma_bulk_load(dst + (size_t)c * pitch, src + (size_t)c * row, row, bar);
-                else
-                    tma_bulk_load(dst, src, (uint32_t)(pf * esz), bar);
-            }
-            c0 += ncopy;
-        }
-    }
     }
     __syncthreads();
     ItemInfo info;
