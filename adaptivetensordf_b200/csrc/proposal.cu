@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kPThreads, 1) proposal_mlp_bwd_kernel(PropMlp 
     const int tid = threadIdx.x, rg = tid % 16, cg = tid / 16;
     // weight-gradient accumulators, kept across tiles
     float g0[4];        // layer 0: k = tid % 16, outputs (tid / 16) * 4 + j
-    float gh[NH][16];   // layers 1..NH: k = tid % 64, outputs (tid / 64) * 16 + j
+    float gh[NH][16];   // layers 1..NH: [4 i + j] = (output cg * 4 + j, input rg + 16 i)
     float gbias[NH + 1];
 #pragma unroll
     for (int j = 0; j < 4; ++j) g0[j] = 0.0f;
@@ -269,11 +269,19 @@ __global__ void __launch_bounds__(kPThreads, 1) proposal_mlp_bwd_kernel(PropMlp 
                     for (int j = 0; j < 4; ++j) g0[j] = fmaf(a, dz[(og * 4 + j) * kPS + r], g0[j]);
                 }
             } else {
-                const int k = tid % kPH, og = tid / kPH;
+                // 4 x 4 outer products per row: 16 FMAs for 8 shared loads (the
+                // inputs rg + 16 i sit 65 floats apart: distinct banks)
+#pragma unroll 4
                 for (int r = 0; r < kPT; ++r) {
-                    const float a = in[k * kPS + r];
+                    float a[4], d[4];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) gh[l - 1][j] = fmaf(a, dz[(og * 16 + j) * kPS + r], gh[l - 1][j]);
+                    for (int i = 0; i < 4; ++i) a[i] = in[(rg + 16 * i) * kPS + r];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) d[j] = dz[(cg * 4 + j) * kPS + r];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) gh[l - 1][4 * i + j] = fmaf(a[i], d[j], gh[l - 1][4 * i + j]);
                 }
             }
             if (tid < kPH) {
@@ -322,13 +330,14 @@ __global__ void __launch_bounds__(kPThreads, 1) proposal_mlp_bwd_kernel(PropMlp 
     }
 #pragma unroll
     for (int l = 1; l <= NH; ++l) {
-        const int k = tid % kPH, og = tid / kPH;
         const int O = l == NH ? kPropOut : kPH;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int o = og * 16 + j;
-            if (o < O) atomicAdd(&m.gw[l][o * kPH + k], gh[l - 1][j]);
-        }
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int o = cg * 4 + j, k = rg + 16 * i;
+                if (o < O) atomicAdd(&m.gw[l][o * kPH + k], gh[l - 1][4 * i + j]);
+            }
     }
     if (tid < kPH) {
 #pragma unroll
