@@ -87,6 +87,21 @@ class MlpGrad(ct.Structure):
     _fields_ = [("weight", ct.c_void_p * MAX_LAYERS), ("bias", ct.c_void_p * MAX_LAYERS)]
 
 
+class ToneMapper(ct.Structure):
+    _fields_ = [
+        ("num_images", ct.c_int32),
+        ("exposure_mode", ct.c_int32),
+        ("exposure", ct.c_void_p),
+        ("sensor_w", ct.c_int32),
+        ("sensor_h", ct.c_int32),
+        ("sensor_bias", ct.c_void_p),
+        ("response_params", ct.c_int32),
+        ("response", ct.c_void_p),
+        ("response_range", ct.c_float),
+        ("leak", ct.c_int32),
+    ]
+
+
 def declared_symbols(header: str = HEADER):
     """Names of the functions include/atdf.h declares."""
     src = open(header).read()
@@ -157,6 +172,9 @@ def _declare(L):
         "atdf_proposal_occupancy": (I32, [P, P, I64, P, P]),
         "atdf_adam_step": (I32, [I64, P, P, P, P, P, F32, F32, F32, F32, F32, I64, P]),
         "atdf_camera_rays": (I32, [I64, P, P, P, P, P, I64, P, I64, I32, I32, I32, I32, P, P, P, P, P]),
+        "atdf_tone_map_forward": (I32, [ct.POINTER(ToneMapper), I64, I64, P, P, P, P, P, P]),
+        "atdf_tone_map_backward": (I32, [ct.POINTER(ToneMapper), I64, I64, P, P, P, P, P, P, P, P, P, P]),
+        "atdf_tone_response_loss": (I32, [I32, P, F32, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

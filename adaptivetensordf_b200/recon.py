@@ -74,6 +74,9 @@ class TiltSeries:
     volume: torch.Tensor     # [N, N, N] float32 phantom (z, y, x), device
     angles: np.ndarray
     image_id: torch.Tensor = None  # [A * P] long: the tilt of each ray
+    uv: torch.Tensor = None        # [A * P, 2] float32: the ray's pixel centre in [0, 1] (u along the width)
+    height: int = 0                # detector size in pixels
+    width: int = 0
 
     @property
     def num_rays(self):
@@ -105,7 +108,10 @@ def make_tilt_series(cfg, device="cuda", noise_seed: int = 1002) -> TiltSeries:
         if cfg.noise > 0:
             sigma = cfg.noise * float(y.max())
             y = y + torch.from_numpy(rng.normal(0.0, sigma, A * P)).to(device)
-    return TiltSeries(o_t, d_t, y.float(), clean, vol_t, angles, torch.from_numpy(img).to(device))
+    n = cfg.detector
+    uv = np.stack([(pix % n + 0.5) / n, (pix // n + 0.5) / n], 1).astype(np.float32)
+    return TiltSeries(o_t, d_t, y.float(), clean, vol_t, angles, torch.from_numpy(img).to(device),
+                      torch.from_numpy(uv).to(device), n, n)
 
 
 # ----------------------------------------------------------------------------
@@ -288,8 +294,9 @@ class TrainOptions:
     start_depth: int = 0        # active depth of the initial tree (0: the config's depth)
     refine_every: int = 0       # epochs between structure refinements (0: none)
     max_active_nodes: int = 0   # leaf budget of the refinement
-    tone_mapper: bool = False   # per-tilt multiplicative exposure (ToneMapper.cpp:161-201)
-    lr_exposure: float = 0.01   # ToneMapper.h:45 exposure_lr
+    tone_mapper: bool = False   # photometric calibration of the projections (ToneMapper.cpp:141-227)
+    tone_params: object = None  # tonemap.PhotometricCalibrationParams (None: the reference's defaults)
+    tone_after_epochs: int = 1  # Settings.h:530 optimize_tone_mapper_after_epochs
     eval_every: int = 0         # steps between evaluations (0: once per epoch)
     target_psnr: float = 30.0
     time_limit: float = 0.0     # seconds of training; 0 = no limit
@@ -365,13 +372,16 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         return a, torch.optim.lr_scheduler.ExponentialLR(a, opt.lr_decay)
 
     adam, sched = make_optimizer(opt.lr_grid, opt.lr_decoder)
-    exposure = None
+    tm = None
     if opt.tone_mapper:
-        # PhotometricCalibration with exposure_mult: the ray integral times the
-        # tilt's exposure factor. The factors are kept at mean 1 after each
-        # step, which fixes the scale that they share with the density.
-        exposure = torch.ones(len(data.angles), device=device, requires_grad=True)
-        adam_exp = torch.optim.Adam([exposure], lr=opt.lr_exposure)
+        # the scene's PhotometricCalibration between the projection and the
+        # loss, with its own SGD / Adam groups (SceneBase.cpp:135-227, 679-694)
+        from .tonemap import PhotometricCalibration
+
+        if data.uv is None:
+            raise ValueError("the tone mapper needs the rays' pixel coordinates (TiltSeries.uv)")
+        tm = PhotometricCalibration(len(data.angles), 1, data.height, data.width, opt.tone_params, device)
+        tm_sgd, tm_adam = tm.make_optimizers()
     prop = None
     if form.endswith("+prop"):
         from .proposal import ProposalSchedule
@@ -393,6 +403,8 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         p = psnr(tree, geo, data.volume) if data.volume is not None else None  # no ground truth: loss only
         rec = {"form": form, "t": t_train, "step": step, "epoch": epoch, "psnr": p,
                "loss": float(loss_acc) / max(1, step)}
+        if tm is not None:
+            rec["exposure_bias"] = tm.exposure_bias.tolist()
         if prop is not None:
             rec.update(prop.stats())
         records.append(rec)
@@ -416,20 +428,23 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
             else:
                 img = geo.ProjectRays(tree, rays, opt.max_samples_per_node, seed)
             pred = img.view(-1)
-            if exposure is not None:
-                pred = pred * exposure[data.image_id[idx]]
+            if tm is not None:
+                pred = tm(pred.view(1, -1), data.uv[idx], data.image_id[idx]).view(-1)
             loss = (pred - target).pow(2).mean()
+            if tm is not None:
+                loss = loss + tm.ParameterLoss().sum()
             if opt.loss_tv > 0:
                 loss = loss + opt.loss_tv * plane_tv(geo.planes)
             adam.zero_grad(set_to_none=True)
-            if exposure is not None:
-                adam_exp.zero_grad(set_to_none=True)
             loss.backward()
             adam.step()
-            if exposure is not None:
-                adam_exp.step()
-                with torch.no_grad():
-                    exposure.div_(exposure.mean())
+            if tm is not None:
+                for o in (tm_sgd, tm_adam):
+                    if o is not None:
+                        if epoch >= opt.tone_after_epochs:
+                            o.step()
+                        o.zero_grad(set_to_none=True)
+                tm.ApplyConstraints()
             loss_acc += loss.detach().double()
             torch.cuda.synchronize()
             t_train += time.perf_counter() - t0

@@ -190,7 +190,7 @@ class Scene:
         if vf.endswith(".npy"):
             vol = torch.from_numpy(np.load(os.path.join(self.path, vf)).astype(np.float32)).to(device)
         angles = self.angles if self.angles is not None else np.zeros(A)
-        return TiltSeries(o, d, y, y.double(), vol, angles, iid)
+        return TiltSeries(o, d, y, y.double(), vol, angles, iid, uv, h, w)
 
 
 def load_scene(path: str) -> Scene:

@@ -22,6 +22,7 @@
  *   hyperacorn/csrc/geometry/geometry.h:269-270        IntegrateSamplesXRay
  *   hyperacorn/csrc/geometry/geometry.h:326-327        AccumulateSampleLossPerNode
  *   hyperacorn/csrc/geometry/geometry.h:335            ComputeImage (fused form)
+ *   hyperacorn/csrc/modules/ToneMapper.cpp:161-201     PhotometricCalibration (tone mapper)
  */
 #ifndef ATDF_H
 #define ATDF_H
@@ -431,6 +432,58 @@ int atdf_camera_rays(int64_t n, const float* uv, const int32_t* image_id, const 
 int atdf_adam_step(int64_t n, float* param, const float* grad, float* exp_avg, float* exp_avg_sq, void* param_bf16,
                    float lr, float beta1, float beta2, float eps, float weight_decay, int64_t step,
                    atdf_stream_t stream);
+
+/* ---- photometric calibration (the tone mapper) ------------------------------
+ * Replaces PhotometricCalibrationImpl::forward
+ * (hyperacorn/csrc/modules/ToneMapper.cpp:161-201) with its camera response
+ * CameraResponseNetImpl::forward (:32-97) and the autograd adjoint of both.
+ * Per element (channel c, ray r) of the projected integrals I [channels, R]:
+ *   x  = I + exposure[image_id[r]]  (ATDF_EXPOSURE_BIAS, exposure_mult = false)
+ *      | I * exposure[image_id[r]]  (ATDF_EXPOSURE_FACTOR, exposure_mult = true)
+ *   x += bilinear(sensor_bias [sensor_h, sensor_w], uv[r])   (border, align_corners = false)
+ *   y  = bilinear(response [response_params], x / range)   (border, align_corners = true)
+ *      + (x - range) when leak and x > range                (training mode)
+ * with torch grid_sample semantics for both lookups; uv [R, 2] in [0, 1]
+ * (u along the width). A disabled part has mode NONE / size 0. The response
+ * curve has one channel: with it, channels must be 1 (ATDF_ERR_UNSUPPORTED
+ * otherwise, as the reference asserts). An image id outside [0, num_images)
+ * sets ATDF_DEVERR_INDEX and yields NaN (forward) / a zero gradient. */
+#define ATDF_EXPOSURE_NONE 0
+#define ATDF_EXPOSURE_BIAS 1
+#define ATDF_EXPOSURE_FACTOR 2
+typedef struct {
+    int32_t num_images;
+    int32_t exposure_mode;    /* ATDF_EXPOSURE_* */
+    const float* exposure;    /* [num_images]: the bias or the factor */
+    int32_t sensor_w, sensor_h; /* sensor-bias map size; 0 = disabled */
+    const float* sensor_bias; /* [sensor_h, sensor_w] */
+    int32_t response_params;  /* samples of the response curve (>= 2); 0 = disabled */
+    const float* response;    /* [response_params] */
+    float response_range;     /* the curve spans inputs [0, range] */
+    int32_t leak;             /* 1: add the leak above the range (training mode) */
+} atdf_tone_mapper_t;
+
+int atdf_tone_map_forward(const atdf_tone_mapper_t* tm, int64_t channels, int64_t num_rays, const float* integral,
+                          const float* uv, const int32_t* image_id, float* out, int32_t* dev_error,
+                          atdf_stream_t stream);
+
+/* The adjoint of atdf_tone_map_forward for grad_out [channels, R]:
+ * grad_integral [channels, R] is written (may be null); grad_exposure
+ * [num_images], grad_sensor_bias [sensor_h, sensor_w] and grad_response
+ * [response_params] are ADDED to (each may be null when not wanted). */
+int atdf_tone_map_backward(const atdf_tone_mapper_t* tm, int64_t channels, int64_t num_rays, const float* integral,
+                           const float* uv, const int32_t* image_id, const float* grad_out, float* grad_integral,
+                           float* grad_exposure, float* grad_sensor_bias, float* grad_response, int32_t* dev_error,
+                           atdf_stream_t stream);
+
+/* The response curve's smoothness loss, CameraResponseNetImpl::ParamLoss
+ * (ToneMapper.cpp:98-111): with f = P sqrt(1e-5) and targets t_0 = 0,
+ * t_{P-1} = range, t_i = (r_{i-1} + r_{i+1}) / 2, loss = sum_i (f r_i - f t_i)^2.
+ * *loss (device float, may be null) is written; (*grad_scale) * d loss / d r
+ * is ADDED to grad_response (may be null); grad_scale is a device float (the
+ * upstream gradient of the loss), null for 1. */
+int atdf_tone_response_loss(int32_t response_params, const float* response, float response_range, float* loss,
+                            float* grad_response, const float* grad_scale, atdf_stream_t stream);
 
 /* ---- forward projection without device allocation ----------------------
  * No counterpart in the reference (it allocates with torch on every call).
