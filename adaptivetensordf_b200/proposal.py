@@ -19,6 +19,16 @@ Judge steps come every judge_every_open steps while the gate is open and
 every judge_every_closed steps while it is closed (every step during the
 first `warmup` steps, to train the proposal). Only the gate's error is read
 back to the host, once per judge step after the warm-up.
+
+The proposal's samples follow a quadrature rule, not an unbiased estimator,
+so its error is a bias that the field learns to fit. With ``residual_gate``
+> 0 (and the batch's targets passed to ``project``) the gate also requires
+that error to stay small beside the current fit: ||proposal - judge|| <=
+residual_gate * ||judge - target||. Early in training the residual is large
+and the proposal runs; once the fit's residual approaches the proposal's
+error the uniform sampler takes over, and while the residual condition
+fails the gate is checked only every judge_every_retired steps (the residual
+keeps falling, so it rarely reopens).
 """
 
 from __future__ import annotations
@@ -29,7 +39,8 @@ import torch
 class ProposalSchedule:
     def __init__(self, tree, geo, max_samples_per_node: int, budget: int = 64, judge_every: int = 10,
                  gate: float = 0.01, lr: float = 3e-3, warmup: int = 20, device: str = "cuda", seed: int = 1005,
-                 jitter: bool = True, judge_every_closed: int = 4, sampler=None):
+                 jitter: bool = True, judge_every_closed: int = 4, sampler=None, residual_gate: float = 0.0,
+                 judge_every_retired: int = 100):
         self.tree, self.geo = tree, geo
         self.M = max_samples_per_node
         if sampler is None:
@@ -51,15 +62,23 @@ class ProposalSchedule:
         self.uniform_steps = 0
         self.last_error = None
         self.last_loss = None
+        self.residual_gate = residual_gate
+        self.judge_every_retired = judge_every_retired
+        self.retired = False        # closed by the residual condition
+        self.last_residual_ratio = None
 
     def is_judge_step(self, step: int) -> bool:
         if step < self.warmup:
             return True
-        every = self.judge_every if self.open else self.judge_every_closed
+        if self.open:
+            every = self.judge_every
+        else:
+            every = self.judge_every_retired if self.retired else self.judge_every_closed
         return step % every == 0
 
-    def project(self, rays, seed: int):
-        """Image of this training step's rays (autograd over the field)."""
+    def project(self, rays, seed: int, target=None):
+        """Image of this training step's rays (autograd over the field);
+        target: the rays' measured projections (for the residual gate)."""
         step = self.step
         self.step += 1
         pseed = seed if self.jitter else 0
@@ -78,12 +97,23 @@ class ProposalSchedule:
             with torch.no_grad():
                 ip = self.ps.Project(self.tree, self.geo, rays, (seed ^ 0x5BD1E995) if self.jitter else 0)
                 ref = img.detach()
-                self.last_error = float((ip - ref).norm() / ref.norm().clamp_min(1e-30))
-            self.open = self.last_error <= self.gate
+                norms = [(ip - ref).norm(), ref.norm()]
+                use_res = self.residual_gate > 0 and target is not None
+                if use_res:
+                    norms.append((ref.reshape(-1) - target.reshape(-1)).norm())
+                vals = torch.stack(norms).tolist()  # one read-back
+            self.last_error = vals[0] / max(vals[1], 1e-30)
+            rel_ok = self.last_error <= self.gate
+            res_ok = True
+            if use_res:
+                self.last_residual_ratio = vals[0] / max(vals[2], 1e-30)
+                res_ok = self.last_residual_ratio <= self.residual_gate
+            self.open = rel_ok and res_ok
+            self.retired = not res_ok
         return img
 
     def stats(self):
         return {"proposal_open": self.open, "proposal_error": self.last_error,
                 "judge_steps": self.judge_steps, "proposal_steps": self.proposal_steps,
-                "uniform_steps": self.uniform_steps,
+                "uniform_steps": self.uniform_steps, "proposal_residual_ratio": self.last_residual_ratio,
                 "proposal_loss": None if self.last_loss is None else float(self.last_loss)}

@@ -290,6 +290,7 @@ class TrainOptions:
     budget: int = 64            # proposal: samples per ray
     gate: float = 0.01          # proposal: relative L2 projection error allowed vs the uniform judge
     judge_every: int = 10       # proposal: steps between judge passes while open
+    residual_gate: float = 0.25  # proposal: its error must stay within this share of the fit residual (0: off)
     proposal_jitter: bool = True  # proposal: jittered (True) or midpoint stratum samples
     start_depth: int = 0        # active depth of the initial tree (0: the config's depth)
     refine_every: int = 0       # epochs between structure refinements (0: none)
@@ -387,6 +388,7 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         from .proposal import ProposalSchedule
 
         prop = ProposalSchedule(tree, geo, opt.max_samples_per_node, budget=opt.budget, gate=opt.gate,
+                                residual_gate=opt.residual_gate,
                                 judge_every=opt.judge_every, device=device, jitter=opt.proposal_jitter)
 
     n = data.num_rays
@@ -424,7 +426,7 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
             target = data.target[idx]
             seed = (step + 1) * 0x9E3779B1
             if prop is not None:
-                img = prop.project(rays, seed)
+                img = prop.project(rays, seed, target)
             else:
                 img = geo.ProjectRays(tree, rays, opt.max_samples_per_node, seed)
             pred = img.view(-1)
@@ -495,6 +497,7 @@ def main():
     ap.add_argument("--budget", type=int, default=64)
     ap.add_argument("--gate", type=float, default=0.01)
     ap.add_argument("--judge-every", type=int, default=10)
+    ap.add_argument("--residual-gate", type=float, default=0.25)
     ap.add_argument("--no-prop-jitter", action="store_true")
     ap.add_argument("--start-depth", type=int, default=0)
     ap.add_argument("--refine-every", type=int, default=0)
@@ -524,7 +527,7 @@ def main():
                        target_psnr=a.target, time_limit=a.time_limit, stop_at_target=not a.no_stop,
                        lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, lr_decay=a.lr_decay, loss_tv=a.tv,
                        init_scale=a.init_scale,
-                       budget=a.budget, gate=a.gate, judge_every=a.judge_every,
+                       budget=a.budget, gate=a.gate, judge_every=a.judge_every, residual_gate=a.residual_gate,
                        proposal_jitter=not a.no_prop_jitter, start_depth=a.start_depth,
                        refine_every=a.refine_every, max_active_nodes=a.max_leaves, tone_mapper=a.tone_mapper)
     recs, reached = train(cfg, a.form, data, opt, log=lambda r: print(json.dumps(r), flush=True))
