@@ -290,7 +290,7 @@ class TrainOptions:
     budget: int = 64            # proposal: samples per ray
     gate: float = 0.01          # proposal: relative L2 projection error allowed vs the uniform judge
     judge_every: int = 10       # proposal: steps between judge passes while open
-    residual_gate: float = 0.25  # proposal: its error must stay within this share of the fit residual (0: off)
+    residual_gate: float = 0.5   # proposal: its error must stay within this share of the fit residual (0: off)
     proposal_jitter: bool = True  # proposal: jittered (True) or midpoint stratum samples
     start_depth: int = 0        # active depth of the initial tree (0: the config's depth)
     refine_every: int = 0       # epochs between structure refinements (0: none)
@@ -497,7 +497,7 @@ def main():
     ap.add_argument("--budget", type=int, default=64)
     ap.add_argument("--gate", type=float, default=0.01)
     ap.add_argument("--judge-every", type=int, default=10)
-    ap.add_argument("--residual-gate", type=float, default=0.25)
+    ap.add_argument("--residual-gate", type=float, default=0.5)
     ap.add_argument("--no-prop-jitter", action="store_true")
     ap.add_argument("--start-depth", type=int, default=0)
     ap.add_argument("--refine-every", type=int, default=0)
