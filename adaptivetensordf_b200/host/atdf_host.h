@@ -171,8 +171,12 @@ class ProposalSampler {
     double mass_mix = 0.25, bin_mix = 0.2, mass_weight = 0.1;
     double mass_power = 0.5, bin_power = 0.5;  // sample density ~ predicted density^power
     bool check_errors = false;  // read the device error words after each call (synchronises)
+    // "fp32": the MLP on CUDA cores in FP32; "bf16": on the tensor cores
+    // (tcgen05, BF16 operands), 3 hidden layers only
+    std::string precision = "fp32";
 
    private:
+    bool tensor_core_mlp() const;
     torch::Tensor logits_for(HyperTreeBase& tree, const atdf_segments_t& view, const RayList& rays,
                              torch::Tensor* features_out);
     torch::Tensor last_ws_, last_bins_, flat_, err_;

@@ -147,7 +147,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def_readwrite("mass_weight", &ProposalSampler::mass_weight)
         .def_readwrite("mass_power", &ProposalSampler::mass_power)
         .def_readwrite("bin_power", &ProposalSampler::bin_power)
-        .def_readwrite("check_errors", &ProposalSampler::check_errors);
+        .def_readwrite("check_errors", &ProposalSampler::check_errors)
+        .def_readwrite("precision", &ProposalSampler::precision);
 
     m.def("IndirectGridSample2D", &IndirectGridSample2D);
     m.def("IndirectGridSample1D", &IndirectGridSample1D);

@@ -779,6 +779,14 @@ ProposalSampler::ProposalSampler(int64_t num_nodes, int64_t hidden, int64_t hidd
     occupancy = torch::zeros({num_nodes, ATDF_PROPOSAL_OCC}, opt.device(torch::Device(device)));
 }
 
+bool ProposalSampler::tensor_core_mlp() const
+{
+    TORCH_CHECK(precision == "fp32" || precision == "bf16", "ProposalSampler.precision: \"fp32\" or \"bf16\"");
+    TORCH_CHECK(precision == "fp32" || weight.size() == 4,
+                "ProposalSampler: the tensor-core MLP (precision \"bf16\") has 3 hidden layers");
+    return precision == "bf16";
+}
+
 std::vector<Tensor> ProposalSampler::parameters() const
 {
     std::vector<Tensor> p;
@@ -806,8 +814,14 @@ Tensor ProposalSampler::logits_for(HyperTreeBase& tree, const atdf_segments_t& v
     flat_ = proposal_flat(weight, bias);
     auto m = mlp_view(dims, flat_.data_ptr<float>(), ATDF_ACT_SILU, ATDF_ACT_ID, 1.0f);
     auto logits = torch::empty({cap, ATDF_PROPOSAL_OUTPUTS}, o.options());
-    check_status(atdf_proposal_mlp_forward(&m, &view, feat.data_ptr<float>(), logits.data_ptr<float>(), stream_arg()),
-                 "atdf_proposal_mlp_forward");
+    if (tensor_core_mlp())
+        check_status(atdf_proposal_mlp_forward_bf16(&m, &view, feat.data_ptr<float>(), logits.data_ptr<float>(),
+                                                    err.data_ptr<int32_t>(), stream_arg()),
+                     "atdf_proposal_mlp_forward_bf16");
+    else
+        check_status(atdf_proposal_mlp_forward(&m, &view, feat.data_ptr<float>(), logits.data_ptr<float>(),
+                                               stream_arg()),
+                     "atdf_proposal_mlp_forward");
     err_ = err;
     if (features_out) *features_out = feat;
     return logits;
@@ -900,9 +914,14 @@ Tensor ProposalSampler::ComputeGradients(HyperTreeBase& tree)
     auto m = mlp_view(dims, flat_.data_ptr<float>(), ATDF_ACT_SILU, ATDF_ACT_ID, 1.0f);
     auto gflat = torch::empty_like(flat_);
     auto gm = mlp_grad_view(dims, gflat.data_ptr<float>());
-    check_status(atdf_proposal_mlp_backward(&m, &view, feat.data_ptr<float>(), dlogits.data_ptr<float>(), &gm,
-                                            stream_arg()),
-                 "atdf_proposal_mlp_backward");
+    if (tensor_core_mlp())
+        check_status(atdf_proposal_mlp_backward_bf16(&m, &view, feat.data_ptr<float>(), dlogits.data_ptr<float>(), &gm,
+                                                     err.data_ptr<int32_t>(), stream_arg()),
+                     "atdf_proposal_mlp_backward_bf16");
+    else
+        check_status(atdf_proposal_mlp_backward(&m, &view, feat.data_ptr<float>(), dlogits.data_ptr<float>(), &gm,
+                                                stream_arg()),
+                     "atdf_proposal_mlp_backward");
     int64_t off = 0;
     for (size_t l = 0; l < weight.size(); ++l) {
         const int64_t nw = weight[l].numel(), nb = bias[l].numel();

@@ -49,6 +49,9 @@ class ProposalSchedule:
             sampler = ProposalSampler(tree.NumNodes(), 64, 3, seed, device)
         self.ps = sampler
         self.ps.budget = budget
+        # the BF16 form runs the proposal MLP on the tensor cores too (3 hidden layers)
+        if getattr(geo, "precision", "fp32") == "bf16" and len(getattr(sampler, "weight", [])) == 4:
+            self.ps.precision = "bf16"
         self.adam = torch.optim.Adam(self.ps.parameters(), lr=lr)
         self.judge_every = judge_every
         self.judge_every_closed = judge_every_closed

@@ -362,6 +362,16 @@ int atdf_proposal_mlp_forward(const atdf_mlp_t* mlp, const atdf_segments_t* segm
 int atdf_proposal_mlp_backward(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
                                const float* grad_logits, const atdf_mlp_grad_t* grad_mlp, atdf_stream_t stream);
 
+/* The same two functions on the tensor cores (tcgen05, BF16 operands, FP32
+ * accumulation) for the 3-hidden-layer network 16 -> 64 -> 64 -> 64 -> 33
+ * (else ATDF_ERR_UNSUPPORTED): results within BF16 rounding of the FP32
+ * kernels above. A bounded wait that runs out sets ATDF_DEVERR_TREE. */
+int atdf_proposal_mlp_forward_bf16(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
+                                   float* logits, int32_t* dev_error, atdf_stream_t stream);
+int atdf_proposal_mlp_backward_bf16(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
+                                    const float* grad_logits, const atdf_mlp_grad_t* grad_mlp, int32_t* dev_error,
+                                    atdf_stream_t stream);
+
 /* Splits a budget of samples per ray over its segments: n = 1 +
  * round((budget - segments of the ray) * share), share = (1 - mass_mix) *
  * weight share + mass_mix * length share, weight = length * (predicted mean

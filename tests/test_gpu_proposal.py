@@ -351,6 +351,80 @@ def test_proposal_mlp_kernels_match_oracle(oracle, hidden_layers):
         assert rel_err(gb[i].cpu().numpy(), db[i]) < REL_TOL, i
 
 
+BF16_TOL = 2e-2  # BF16 operands, FP32 accumulation
+
+
+def _mlp_struct(ps):
+    from adaptivetensordf_b200 import capi
+
+    m = capi.Mlp()
+    ws = [w.detach().contiguous() for w in ps.weight]
+    bs = [b.detach().contiguous() for b in ps.bias]
+    m.num_layers = len(ws)
+    m.dims[0] = po.INPUTS
+    for i, w in enumerate(ws):
+        m.dims[i + 1] = w.shape[0]
+        m.weight[i] = w.data_ptr()
+        m.bias[i] = bs[i].data_ptr()
+    m.hidden_activation = capi.ACT["silu"]
+    m.last_activation = capi.ACT["id"]
+    m.softplus_beta = 1.0
+    return m, ws, bs
+
+
+@pytest.mark.parametrize("R", [700, 12000])
+def test_proposal_mlp_tensor_core_kernels(oracle, R):
+    """The tcgen05 proposal MLP (BF16 operands, FP32 accumulation in TMEM)
+    against the oracle's FP64 MLP: logits and weight / bias gradients within
+    the BF16 tolerance, over a row count read on the device (12000 rays give
+    several 128-row tiles per CTA, accumulated in TMEM); rows past the count
+    untouched; a 1-hidden-layer network is refused."""
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import capi
+
+    tree, geo, o, d = gpu_scene(3, 8, 9, (64, 9, 64), [32], R, seed=4)
+    pl = Placed(tree, geo, o, d, 1)
+    G = int(pl.totals()[0])
+    ps = ab.ProposalSampler(tree.NumNodes(), 64, 3, 11, "cuda")
+    with torch.no_grad():  # a trained-looking last layer (the init scales it by 0.1)
+        ps.weight[3].mul_(10.0)
+    rng = np.random.default_rng(5)
+    x = rng.normal(size=(pl.view.capacity, po.INPUTS)).astype(np.float32)
+    md = {"layers": [(w.detach().cpu().numpy(), b.detach().cpu().numpy()) for w, b in zip(ps.weight, ps.bias)],
+          "act": "silu", "last_act": "id", "beta": 1.0}
+    L = capi.lib()
+    m, ws, bs = _mlp_struct(ps)
+    xd = torch.from_numpy(x).cuda()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = torch.full((pl.view.capacity, po.OUTPUTS), 7.0, device="cuda")
+    assert L.atdf_proposal_mlp_forward_bf16(ct.byref(m), ct.byref(pl.view), capi.ptr(xd), capi.ptr(out),
+                                            capi.ptr(err), None) == 0
+    torch.cuda.synchronize()
+    ref = oracle.mlp_forward(md, x[:G], np.float64)
+    assert rel_err(out[:G].cpu().numpy(), ref) < BF16_TOL
+    assert torch.all(out[G:] == 7.0)
+    g = rng.normal(size=(pl.view.capacity, po.OUTPUTS))
+    gw = [torch.full_like(w, 3.0) for w in ws]
+    gb = [torch.full_like(b, 3.0) for b in bs]
+    mg = capi.MlpGrad()
+    for i in range(len(ws)):
+        mg.weight[i] = gw[i].data_ptr()
+        mg.bias[i] = gb[i].data_ptr()
+    gd = torch.from_numpy(g.astype(np.float32)).cuda()
+    assert L.atdf_proposal_mlp_backward_bf16(ct.byref(m), ct.byref(pl.view), capi.ptr(xd), capi.ptr(gd),
+                                             ct.byref(mg), capi.ptr(err), None) == 0
+    torch.cuda.synchronize()
+    dW, db, _ = oracle.mlp_backward(md, x[:G], g[:G], np.float64)
+    for i in range(len(ws)):
+        assert rel_err(gw[i].cpu().numpy(), dW[i]) < BF16_TOL, i
+        assert rel_err(gb[i].cpu().numpy(), db[i]) < BF16_TOL, i
+    assert int(err.item()) == 0
+    ps1 = ab.ProposalSampler(tree.NumNodes(), 64, 1, 11, "cuda")
+    m1, _, _ = _mlp_struct(ps1)
+    assert L.atdf_proposal_mlp_forward_bf16(ct.byref(m1), ct.byref(pl.view), capi.ptr(xd), capi.ptr(out),
+                                            capi.ptr(err), None) == 2  # ATDF_ERR_UNSUPPORTED
+
+
 def test_proposal_projection_converges():
     """Projections through a random (untrained) proposal converge to the
     dense uniform projection as the budget grows."""
