@@ -92,7 +92,14 @@ __device__ __forceinline__ void st8(unsigned char* dst, const float* v)
                                                  pack2(v[6], v[7]));
 }
 
-__device__ __forceinline__ float sig(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// Logistic function from the hardware tanh approximation (one MUFU op,
+// ~2^-11 relative error, below the BF16 rounding of the activations).
+__device__ __forceinline__ float sig(float z)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(0.5f * z));
+    return fmaf(0.5f, y, 0.5f);
+}
 __device__ __forceinline__ float silu_f(float z) { return z * sig(z); }
 __device__ __forceinline__ float dsilu(float z)
 {
@@ -101,19 +108,40 @@ __device__ __forceinline__ float dsilu(float z)
 }
 
 // Weights as BF16 K-major [out][in] (W3 padded to 64 rows), biases FP32.
+// Four consecutive inputs per load (rows of 16 or 64 floats, 16-byte
+// aligned), eight loads in flight per thread: this runs once per CTA, and a
+// chain of dependent global loads here would cost more than a tile.
 __device__ void load_weights(const Mlp4& m, unsigned char* sm, int nthreads)
 {
-    const int K[4] = {kIn, kH, kH, kH};
-    const uint32_t off[4] = {kW0, kW1, kW2, kW3};
-    for (int l = 0; l < 4; ++l) {
-        const int O = l == 3 ? kOut : kH, Kl = K[l];
-        for (int e = threadIdx.x; e < kH * Kl; e += nthreads) {
-            const int n = e / Kl, k = e % Kl;
-            const float v = n < O ? m.w[l][n * Kl + k] : 0.0f;
-            *reinterpret_cast<__nv_bfloat16*>(sm + off[l] + tc::kmajor_off(n, k, Kl)) = __float2bfloat16_rn(v);
+    constexpr int kQ0 = kH * kIn / 4, kQh = kH * kH / 4, kQ = kQ0 + 3 * kQh;  // float4s of W0 and W1..W3
+    for (int e0 = threadIdx.x; e0 < kQ; e0 += 8 * nthreads) {
+        float4 v[8];
+        int l[8], n[8], k[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * nthreads;
+            l[u] = e < kQ0 ? 0 : 1 + (e - kQ0) / kQh;
+            const int Kl = l[u] == 0 ? kIn : kH;
+            const int q = l[u] == 0 ? e : (e - kQ0) % kQh;
+            n[u] = (4 * q) / Kl;
+            k[u] = (4 * q) % Kl;
+            const int O = l[u] == 3 ? kOut : kH;
+            v[u] = (e < kQ && n[u] < O) ? *reinterpret_cast<const float4*>(m.w[l[u]] + n[u] * Kl + k[u])
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        float* b = reinterpret_cast<float*>(sm + kBias) + l * kH;
-        for (int o = threadIdx.x; o < kH; o += nthreads) b[o] = o < O ? m.b[l][o] : 0.0f;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (e0 + u * nthreads >= kQ) continue;
+            const uint32_t off = l[u] == 0 ? kW0 : l[u] == 1 ? kW1 : l[u] == 2 ? kW2 : kW3;
+            const int Kl = l[u] == 0 ? kIn : kH;
+            *reinterpret_cast<uint2*>(sm + off + tc::kmajor_off(n[u], k[u], Kl)) =
+                make_uint2(pack2(v[u].x, v[u].y), pack2(v[u].z, v[u].w));
+        }
+    }
+    float* b = reinterpret_cast<float*>(sm + kBias);
+    for (int i = threadIdx.x; i < 4 * kH; i += nthreads) {
+        const int l = i / kH, o = i % kH;
+        b[i] = o < (l == 3 ? kOut : kH) ? m.b[l][o] : 0.0f;
     }
 }
 
@@ -226,16 +254,21 @@ __global__ void __launch_bounds__(kRows) prop_tc_forward_kernel(Mlp4 m, const in
     const int64_t nrows = *count;
     uint32_t phase = 0;
     bool alive = true;
-    for (int64_t row0 = (int64_t)blockIdx.x * kRows; alive && row0 < nrows; row0 += (int64_t)gridDim.x * kRows) {
-        const int64_t row = row0 + t;
-        float v[16];
+    // this thread's row of the next tile, loaded while the current one runs
+    float v[16];
+    auto fetch = [&](int64_t r0) {
+        const int64_t row = r0 + t;
         if (row < nrows)
             ld16(x + row * kIn, v);
         else
 #pragma unroll
             for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+    };
+    fetch((int64_t)blockIdx.x * kRows);
+    for (int64_t row0 = (int64_t)blockIdx.x * kRows; alive && row0 < nrows; row0 += (int64_t)gridDim.x * kRows) {
         st8(sm + kFX + tc::kmajor_off(t, 0, kIn), v);
         st8(sm + kFX + tc::kmajor_off(t, 8, kIn), v + 8);
+        fetch(row0 + (int64_t)gridDim.x * kRows);
 #pragma unroll 1
         for (int l = 0; l < 4; ++l) {
             to_async_and_sync();
@@ -307,24 +340,23 @@ __global__ void __launch_bounds__(2 * kRows, 1) prop_tc_backward_kernel(Mlp4 m, 
     const int c0 = 32 * h;  // this thread's half of a 64-column layer
     uint32_t phase = 0;
     bool alive = true, had_tile = false;
-    for (int64_t row0 = (int64_t)blockIdx.x * kRows; alive && row0 < nrows; row0 += (int64_t)gridDim.x * kRows) {
-        const int64_t row = row0 + t;
+    // this thread's X half (8 features) and dZ3 half (32 logits, zero past
+    // 33) of the next tile, loaded while the current one runs
+    float xv[8], gv[32];
+    auto fetch = [&](int64_t r0) {
+        const int64_t row = r0 + t;
         const bool in = row < nrows;
-        {  // X half (8 features) and dZ3 half (32 logits, zero past 33)
-            float v[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = in ? x[row * kIn + 8 * h + i] : 0.0f;
-            st8(HBQ + tc::kmajor_off(t, 64 + 8 * h, kHBQ), v);
+        for (int i = 0; i < 8; ++i) xv[i] = in ? x[row * kIn + 8 * h + i] : 0.0f;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+        for (int i = 0; i < 32; ++i) gv[i] = (in && c0 + i < kOut) ? gout[row * kOut + c0 + i] : 0.0f;
+    };
+    fetch((int64_t)blockIdx.x * kRows);
+    for (int64_t row0 = (int64_t)blockIdx.x * kRows; alive && row0 < nrows; row0 += (int64_t)gridDim.x * kRows) {
+        st8(HBQ + tc::kmajor_off(t, 64 + 8 * h, kHBQ), xv);
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int c = c0 + 8 * q + i;
-                    v[i] = (in && c < kOut) ? gout[row * kOut + c] : 0.0f;
-                }
-                st8(GP + tc::kmajor_off(t, c0 + 8 * q, kG), v);
-            }
-        }
+        for (int q = 0; q < 4; ++q) st8(GP + tc::kmajor_off(t, c0 + 8 * q, kG), gv + 8 * q);
+        fetch(row0 + (int64_t)gridDim.x * kRows);
         // forward: Z0, Z1, Z2 into TMEM, A0 -> HBQ, A1 -> HBP[64..], A2 -> HBP[0..]
         to_async_and_sync();
         if (tid == 0) {
@@ -441,6 +473,8 @@ __global__ void __launch_bounds__(2 * kRows, 1) prop_tc_backward_kernel(Mlp4 m, 
     if (tid < 32) tc::tmem_dealloc(s_tmem, kTmemBwd);
 }
 
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 static int check_mlp(const atdf_mlp_t* m)
 {
     if (!m || m->num_layers != 4 || m->dims[0] != kIn || m->dims[4] != kOut) return ATDF_ERR_UNSUPPORTED;
@@ -448,7 +482,7 @@ static int check_mlp(const atdf_mlp_t* m)
         if (m->dims[l] != kH) return ATDF_ERR_UNSUPPORTED;
     if (m->hidden_activation != ATDF_ACT_SILU || m->last_activation != ATDF_ACT_ID) return ATDF_ERR_UNSUPPORTED;
     for (int l = 0; l < 4; ++l)
-        if (!m->weight[l] || !m->bias[l]) return ATDF_ERR_INVALID_ARGUMENT;
+        if (!m->weight[l] || !m->bias[l] || !aligned16(m->weight[l])) return ATDF_ERR_INVALID_ARGUMENT;
     return ATDF_OK;
 }
 
@@ -471,7 +505,8 @@ extern "C" {
 int atdf_proposal_mlp_forward_bf16(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
                                    float* logits, int32_t* dev_error, atdf_stream_t stream)
 {
-    if (!segments || !segments->totals || !features || !logits || !dev_error) return ATDF_ERR_INVALID_ARGUMENT;
+    if (!segments || !segments->totals || !features || !logits || !dev_error || !aligned16(features))
+        return ATDF_ERR_INVALID_ARGUMENT;
     int st = check_mlp(mlp);
     if (st != ATDF_OK) return st;
     Mlp4 m{};

@@ -206,6 +206,7 @@ def measure_proposal(args, tree, cfg, dev_batches, nb, stream):
     opt = Adam(params, lr=1e-3, geometry=geo)  # also writes the BF16 working copies
     ps = ab.ProposalSampler(tree.NumNodes(), 64, 3, 1005, "cuda")
     ps.budget = 128
+    ps.precision = "bf16"  # the proposal MLP on the tensor cores, as in the BF16 form's schedule
     padam = torch.optim.Adam(ps.parameters(), lr=3e-3)
 
     def step(k, judge):

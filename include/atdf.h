@@ -365,7 +365,9 @@ int atdf_proposal_mlp_backward(const atdf_mlp_t* mlp, const atdf_segments_t* seg
 /* The same two functions on the tensor cores (tcgen05, BF16 operands, FP32
  * accumulation) for the 3-hidden-layer network 16 -> 64 -> 64 -> 64 -> 33
  * (else ATDF_ERR_UNSUPPORTED): results within BF16 rounding of the FP32
- * kernels above. A bounded wait that runs out sets ATDF_DEVERR_TREE. */
+ * kernels above. The weights and the features must be 16-byte aligned
+ * (ATDF_ERR_INVALID_ARGUMENT otherwise). A bounded wait that runs out sets
+ * ATDF_DEVERR_TREE. */
 int atdf_proposal_mlp_forward_bf16(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
                                    float* logits, int32_t* dev_error, atdf_stream_t stream);
 int atdf_proposal_mlp_backward_bf16(const atdf_mlp_t* mlp, const atdf_segments_t* segments, const float* features,
