@@ -374,8 +374,10 @@ def run_ours(args, rank, world):
         clocks = sampler.stop() if sampler else None
         # forward and backward calls timed alone (CUDA events on the launching
         # stream). The calls are enqueued back to back with no host
-        # synchronisation in between, so the host runs ahead of the GPU and each
-        # event pair brackets the call's GPU work only.
+        # synchronisation in between, and two more forward passes (no autograd)
+        # are queued between a forward and its backward, so the GPU still has
+        # work queued while the host runs the autograd engine's part of the
+        # backward call: each event pair brackets the call's GPU work only.
         reps = 5
         o, d, y = dev_batches[0]
         rays = ab.RayList(o, d)
@@ -387,6 +389,9 @@ def run_ours(args, rank, world):
             img = geo.ProjectRays(tree, rays, M, 7)
             f1.record(stream)
             gimg = torch.ones_like(img)
+            with torch.no_grad():
+                for _ in range(2):
+                    geo.ProjectRays(tree, rays, M, 7)
             b0.record(stream)
             img.backward(gimg)
             b1.record(stream)
