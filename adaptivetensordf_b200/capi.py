@@ -87,6 +87,23 @@ class MlpGrad(ct.Structure):
     _fields_ = [("weight", ct.c_void_p * MAX_LAYERS), ("bias", ct.c_void_p * MAX_LAYERS)]
 
 
+class AdamTensor(ct.Structure):
+    _fields_ = [
+        ("n", ct.c_int64),
+        ("param", ct.c_void_p),
+        ("grad", ct.c_void_p),
+        ("exp_avg", ct.c_void_p),
+        ("exp_avg_sq", ct.c_void_p),
+        ("param_bf16", ct.c_void_p),
+        ("lr", ct.c_float),
+        ("beta1", ct.c_float),
+        ("beta2", ct.c_float),
+        ("eps", ct.c_float),
+        ("weight_decay", ct.c_float),
+        ("step", ct.c_int64),
+    ]
+
+
 class ToneMapper(ct.Structure):
     _fields_ = [
         ("num_images", ct.c_int32),
@@ -174,6 +191,7 @@ def _declare(L):
         "atdf_proposal_loss": (I32, [ct.POINTER(Segments), P, P, P, F32, P, P, P, P, I64, P, P]),
         "atdf_proposal_occupancy": (I32, [P, P, I64, P, P]),
         "atdf_adam_step": (I32, [I64, P, P, P, P, P, F32, F32, F32, F32, F32, I64, P]),
+        "atdf_adam_step_multi": (I32, [I32, P, P]),
         "atdf_camera_rays": (I32, [I64, P, P, P, P, P, I64, P, I64, I32, I32, I32, I32, P, P, P, P, P]),
         "atdf_tone_map_forward": (I32, [ct.POINTER(ToneMapper), I64, I64, P, P, P, P, P, P]),
         "atdf_tone_map_backward": (I32, [ct.POINTER(ToneMapper), I64, I64, P, P, P, P, P, P, P, P, P, P]),

@@ -4,9 +4,10 @@ The BF16 form projects from BF16 copies of the FP32 factor planes and lines
 (``GeometryTensorQO.RefreshLowPrecision``). With ``torch.optim.Adam`` a
 training step updates the FP32 masters and then casts them again, a second
 pass over 227 MB of planes on the C2 workload. ``Adam`` here performs the same
-update (torch.optim.Adam's, no amsgrad) through ``atdf_adam_step``, one kernel
-per parameter that also writes the parameter's BF16 copy, so no
-``RefreshLowPrecision`` is needed after ``step()``.
+update (torch.optim.Adam's, no amsgrad) through ``atdf_adam_step_multi``:
+every parameter in one launch (a block range per parameter), which also
+writes each parameter's BF16 copy, so no ``RefreshLowPrecision`` is needed
+after ``step()``.
 
 The reference trains the grid and decoder with ``torch::optim::Adam``
 (hyperacorn/csrc/geometry/geometry_tensor_qo.cpp:79-81, 209-220).
@@ -60,6 +61,7 @@ class Adam(torch.optim.Optimizer):
         L = capi.lib()
         stream = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
         twins = self._twins()
+        batch, keep, copies = [], [], []  # one atdf_adam_step_multi call for every parameter
         for group in self.param_groups:
             b1, b2 = group["betas"]
             for p in group["params"]:
@@ -82,12 +84,22 @@ class Adam(torch.optim.Optimizer):
                     g = g.contiguous(memory_format=torch.preserve_format)
                     if g.stride() != p.stride():
                         raise RuntimeError("Adam: gradient and parameter layouts differ")
-                status = L.atdf_adam_step(p.numel(), capi.ptr(p), capi.ptr(g), capi.ptr(st["exp_avg"]),
-                                          capi.ptr(st["exp_avg_sq"]), capi.ptr(twin) if fused_twin else None,
-                                          float(group["lr"]), float(b1), float(b2), float(group["eps"]),
-                                          float(group["weight_decay"]), int(st["step"]), stream)
-                if status != 0:
-                    raise RuntimeError(f"atdf_adam_step: {L.atdf_status_string(status).decode()}")
+                t = capi.AdamTensor()
+                t.n = p.numel()
+                t.param, t.grad = p.data_ptr(), g.data_ptr()
+                t.exp_avg, t.exp_avg_sq = st["exp_avg"].data_ptr(), st["exp_avg_sq"].data_ptr()
+                t.param_bf16 = twin.data_ptr() if fused_twin else None
+                t.lr, t.beta1, t.beta2 = float(group["lr"]), float(b1), float(b2)
+                t.eps, t.weight_decay, t.step = float(group["eps"]), float(group["weight_decay"]), int(st["step"])
+                batch.append(t)
+                keep.append(g)
                 if twin is not None and not fused_twin:
-                    twin.copy_(p)
+                    copies.append((twin, p))
+        if batch:
+            arr = (capi.AdamTensor * len(batch))(*batch)
+            status = L.atdf_adam_step_multi(len(batch), arr, stream)
+            if status != 0:
+                raise RuntimeError(f"atdf_adam_step_multi: {L.atdf_status_string(status).decode()}")
+        for twin, p in copies:
+            twin.copy_(p)
         return loss

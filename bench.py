@@ -424,8 +424,8 @@ def run_ours(args, rank, world):
     if rank != 0:
         return
     # this library's kernels per uniform training step of the BF16 form: 13 for
-    # sampling, bucketing, projection and loss, 12 Adam steps (one per parameter)
-    launches_per_step = 25
+    # sampling, bucketing, projection and loss, and one Adam launch for the 12 parameters
+    launches_per_step = 14
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
     # tcgen05 backward launch on this workload at 16384 rays, from a
     # single-pass ncu capture of the bench's warm-up step; the gradient

@@ -445,6 +445,20 @@ int atdf_adam_step(int64_t n, float* param, const float* grad, float* exp_avg, f
                    float lr, float beta1, float beta2, float eps, float weight_decay, int64_t step,
                    atdf_stream_t stream);
 
+/* atdf_adam_step for `count` parameter tensors (each with its own sizes,
+ * hyper-parameters and step) in one launch per 16 tensors. */
+typedef struct {
+    int64_t n;
+    float* param;
+    const float* grad;
+    float* exp_avg;
+    float* exp_avg_sq;
+    void* param_bf16; /* nullable */
+    float lr, beta1, beta2, eps, weight_decay;
+    int64_t step;
+} atdf_adam_tensor_t;
+int atdf_adam_step_multi(int32_t count, const atdf_adam_tensor_t* tensors, atdf_stream_t stream);
+
 /* ---- photometric calibration (the tone mapper) ------------------------------
  * Replaces PhotometricCalibrationImpl::forward
  * (hyperacorn/csrc/modules/ToneMapper.cpp:161-201) with its camera response

@@ -93,3 +93,41 @@ def test_fused_adam_writes_the_bf16_copies():
     for m in range(3):
         assert torch.equal(geo.planes_bf16[m], geo.planes[m].detach().to(torch.bfloat16))
         assert torch.equal(geo.lines_bf16[m], geo.lines[m].detach().to(torch.bfloat16))
+
+
+def test_single_tensor_entry_equals_the_batched_launch():
+    """atdf_adam_step (one tensor per call) and atdf_adam_step_multi (every
+    tensor in one launch, here 20 tensors: two launches of at most 16) apply
+    the same arithmetic, so their results are identical."""
+    import ctypes as ct
+
+    from adaptivetensordf_b200 import capi
+
+    L = capi.lib()
+    g = torch.Generator(device="cpu").manual_seed(3)
+    sizes = [1, 3, 5, 64, 1023, 4096, 70001] * 3
+    sizes = sizes[:20]
+    mk = lambda n: torch.randn(n, generator=g).cuda()  # noqa: E731
+    a = [[mk(n) for _ in range(4)] for n in sizes]  # param, grad, m, v
+    for t in a:
+        t[3].abs_()
+    b = [[x.clone() for x in t] for t in a]
+    pb = [torch.empty(n, dtype=torch.bfloat16, device="cuda") for n in sizes]
+    stream = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for (p, gr, m, v), q in zip(a, pb):
+        assert L.atdf_adam_step(p.numel(), capi.ptr(p), capi.ptr(gr), capi.ptr(m), capi.ptr(v), capi.ptr(q), 3e-3,
+                                0.9, 0.999, 1e-8, 0.01, 7, stream) == 0
+    arr = (capi.AdamTensor * len(sizes))()
+    pb2 = [torch.empty_like(q) for q in pb]
+    for i, ((p, gr, m, v), q) in enumerate(zip(b, pb2)):
+        t = arr[i]
+        t.n, t.param, t.grad, t.exp_avg, t.exp_avg_sq, t.param_bf16 = (p.numel(), p.data_ptr(), gr.data_ptr(),
+                                                                         m.data_ptr(), v.data_ptr(), q.data_ptr())
+        t.lr, t.beta1, t.beta2, t.eps, t.weight_decay, t.step = 3e-3, 0.9, 0.999, 1e-8, 0.01, 7
+    assert L.atdf_adam_step_multi(len(sizes), arr, stream) == 0
+    torch.cuda.synchronize()
+    for ta, tb in zip(a, b):
+        for x, y in zip(ta, tb):
+            assert torch.equal(x, y)
+    for q, q2 in zip(pb, pb2):
+        assert torch.equal(q, q2)
