@@ -125,9 +125,13 @@ struct GeometryTensorQO {
     torch::Tensor SampleVolumeIndirect_feature(HyperTreeBase& tree, torch::Tensor global_coordinate,
                                                torch::Tensor node_id);
     torch::Tensor SampleVolumeIndirect(HyperTreeBase& tree, torch::Tensor global_coordinate, torch::Tensor node_id);
-    // HierarchicalNeuralGeometry::ComputeImage (geometry.h:335), unfused.
-    torch::Tensor ComputeImage(HyperTreeBase& tree, const SampleList& samples, int num_channels,
-                               int64_t num_pixels);
+    // HierarchicalNeuralGeometry::ComputeImage (geometry.h:335, geometry.cpp:
+    // 828-914), unfused: (image [C, R], ratio, ratio_inv). As in the
+    // reference's indirect-sampling path, ratio and ratio_inv are undefined
+    // and use_decoder has no effect (it only steers the batched path).
+    std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> ComputeImage(HyperTreeBase& tree,
+                                                                         const SampleList& samples, int num_channels,
+                                                                         int64_t num_pixels, bool use_decoder = true);
     // Fused forward projection with the hand-written adjoint.
     torch::Tensor ProjectRays(HyperTreeBase& tree, const RayList& rays, int max_samples_per_node,
                               uint64_t jitter_seed);

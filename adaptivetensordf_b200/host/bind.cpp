@@ -122,7 +122,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
             [](GeometryTensorQO& g, double v) { g.decoder.softplus_beta = v; })
         .def("SampleVolumeIndirect_feature", &GeometryTensorQO::SampleVolumeIndirect_feature)
         .def("SampleVolumeIndirect", &GeometryTensorQO::SampleVolumeIndirect)
-        .def("ComputeImage", &GeometryTensorQO::ComputeImage)
+        .def("ComputeImage", &GeometryTensorQO::ComputeImage, py::arg("tree"), py::arg("samples"),
+             py::arg("num_channels"), py::arg("num_pixels"), py::arg("use_decoder") = true)
         .def("ProjectRays", &GeometryTensorQO::ProjectRays, py::arg("tree"), py::arg("rays"),
              py::arg("max_samples_per_node"), py::arg("jitter_seed") = 0)
         .def("ProjectNodeError", &GeometryTensorQO::ProjectNodeError, py::arg("tree"), py::arg("rays"),

@@ -549,11 +549,14 @@ Tensor GeometryTensorQO::SampleVolumeIndirect(HyperTreeBase& tree, Tensor global
     return DecodeFeatures(decoder, feat).contiguous();
 }
 
-Tensor GeometryTensorQO::ComputeImage(HyperTreeBase& tree, const SampleList& samples, int num_channels,
-                                      int64_t num_pixels)
+std::tuple<Tensor, Tensor, Tensor> GeometryTensorQO::ComputeImage(HyperTreeBase& tree, const SampleList& samples,
+                                                                  int num_channels, int64_t num_pixels,
+                                                                  bool use_decoder)
 {
+    (void)use_decoder;
     auto out = SampleVolumeIndirect(tree, samples.global_coordinate, samples.node_id);
-    return IntegrateSamplesXRay(out, samples.weight.unsqueeze(1), samples.ray_index, num_channels, num_pixels);
+    auto image = IntegrateSamplesXRay(out, samples.weight.unsqueeze(1), samples.ray_index, num_channels, num_pixels);
+    return {image, Tensor(), Tensor()};
 }
 
 static atdf_field_t fused_field_view(const GeometryTensorQO& g, const std::vector<Tensor>& planes,

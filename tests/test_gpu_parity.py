@@ -151,7 +151,8 @@ def test_unfused_field_decoder_integral(oracle, tensor_op):
     feat = geo.SampleVolumeIndirect_feature(tree, s.global_coordinate, s.node_id)
     feat_o = oracle.vm_features(fd, td, so["global_coordinate"], so["node_id"], np.float32)
     assert np.array_equal(feat.detach().cpu().numpy(), feat_o)
-    img = geo.ComputeImage(tree, s, 1, R)
+    img, ratio, ratio_inv = geo.ComputeImage(tree, s, 1, R)
+    assert ratio is None and ratio_inv is None  # undefined, as in the reference's indirect path
     img_o = oracle.project_forward(fd, md, td, so, R, np.float64)
     assert rel_err(img.detach().cpu().numpy(), img_o) < REL_TOL
     gi = np.random.default_rng(3).normal(size=img_o.shape)

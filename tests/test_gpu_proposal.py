@@ -506,3 +506,38 @@ def test_trained_proposal_beats_uniform_sampling():
     assert n_uni >= 64
     assert e_prop < 0.85 * e_same
     assert e_prop < e_uni
+
+
+def test_proposal_mlp_tensor_core_kernels_with_no_segments():
+    """A batch whose rays all miss the tree has no segments: the tensor-core
+    kernels read the zero count on the device and do nothing (logits
+    untouched, gradients zero)."""
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import capi
+
+    tree, geo, o, d = gpu_scene(2, 8, 9, (16, 9, 16), [32], 64, seed=1)
+    o = np.tile(np.array([[5.0, 5.0, 5.0]], np.float32), (64, 1))
+    d = np.tile(np.array([[0.0, 0.0, 1.0]], np.float32), (64, 1))
+    pl = Placed(tree, geo, o, d, 1)
+    assert int(pl.totals()[0]) == 0
+    ps = ab.ProposalSampler(tree.NumNodes(), 64, 3, 3, "cuda")
+    L = capi.lib()
+    m, ws, bs = _mlp_struct(ps)
+    cap = max(pl.view.capacity, 1)
+    xd = torch.zeros(cap, po.INPUTS, device="cuda")
+    out = torch.full((cap, po.OUTPUTS), 7.0, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert L.atdf_proposal_mlp_forward_bf16(ct.byref(m), ct.byref(pl.view), capi.ptr(xd), capi.ptr(out),
+                                            capi.ptr(err), None) == 0
+    gw = [torch.full_like(w, 3.0) for w in ws]
+    gb = [torch.full_like(b, 3.0) for b in bs]
+    mg = capi.MlpGrad()
+    for i in range(len(ws)):
+        mg.weight[i] = gw[i].data_ptr()
+        mg.bias[i] = gb[i].data_ptr()
+    gd = torch.zeros(cap, po.OUTPUTS, device="cuda")
+    assert L.atdf_proposal_mlp_backward_bf16(ct.byref(m), ct.byref(pl.view), capi.ptr(xd), capi.ptr(gd),
+                                             ct.byref(mg), capi.ptr(err), None) == 0
+    torch.cuda.synchronize()
+    assert torch.all(out == 7.0) and int(err.item()) == 0
+    assert all(float(t.abs().sum()) == 0.0 for t in gw + gb)

@@ -138,3 +138,16 @@ def test_training_with_the_tone_mapper():
     bias = recs[-1]["exposure_bias"]
     assert min(bias) >= 0.0
     assert np.corrcoef(bias, offs.cpu().numpy())[0, 1] > 0.5
+
+
+def test_empty_batch():
+    """No rays: nothing is launched, the outputs are empty and the parameter
+    gradients stay zero."""
+    from adaptivetensordf_b200 import tonemap
+
+    m = tonemap.PhotometricCalibration(3, 1, 32, 32)
+    x = torch.zeros(1, 0, device="cuda", requires_grad=True)
+    y = m(x, torch.zeros(0, 2, device="cuda"), torch.zeros(0, dtype=torch.long, device="cuda"))
+    assert y.shape == (1, 0)
+    y.sum().backward()
+    assert float(m.exposure_bias.grad.abs().sum()) == 0.0 and float(m.sensor_bias.grad.abs().sum()) == 0.0
