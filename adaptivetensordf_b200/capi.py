@@ -172,6 +172,8 @@ def _declare(L):
                                                U64, P, P, P]),
         "atdf_siddon_project": (I32, [P, I32, I32, I32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), P, P,
                                       I64, P, P]),
+        "atdf_project_forward_segmented": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, U64,
+                                                 P, P, SZ, P, P]),
         "atdf_project_forward_binned": (I32, [ct.POINTER(Tree), ct.POINTER(Field), ct.POINTER(Mlp), P, P, I64, I32,
                                               U64, P, P, P, SZ, P, P]),
         "atdf_project_segments": (I32, [ct.POINTER(Tree), P, P, I64, I32, I64, P, SZ, ct.POINTER(Segments), P, P]),

@@ -1023,6 +1023,15 @@ int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, con
                            (cudaStream_t)stream);
 }
 
+int atdf_project_forward_segmented(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                   const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                   uint64_t jitter_seed, float* image, void* workspace, size_t workspace_bytes,
+                                   int32_t* dev_error, atdf_stream_t stream)
+{
+    return project_forward(tree, field, mlp, ray_origin, ray_direction, num_rays, 0, jitter_seed, false, nullptr,
+                           nullptr, nullptr, image, workspace, workspace_bytes, dev_error, (cudaStream_t)stream);
+}
+
 int atdf_project_forward_binned(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
                                 const float* ray_origin, const float* ray_direction, int64_t num_rays,
                                 int32_t max_samples_per_node, uint64_t jitter_seed, float* image, float* seg_bins,

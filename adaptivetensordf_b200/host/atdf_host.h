@@ -119,6 +119,11 @@ struct GeometryTensorQO {
     // cores; gradients still flow to the FP32 parameters.
     std::string precision = "fp32";
     std::vector<torch::Tensor> planes_bf16, lines_bf16;
+    // A cudaEvent_t (as an integer; 0 = none) that marks the end of the last
+    // parameter update when that update ran on another stream (an optimizer
+    // step). ProjectRays then runs the ray/leaf segment pass, which does not
+    // read the parameters, before the current stream waits for the event.
+    int64_t params_ready = 0;
     void RefreshLowPrecision();
 
     atdf_field_t view() const;

@@ -102,6 +102,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def_readwrite("roi_max", &GeometryTensorQO::roi_max)
         .def_readwrite("tensor_op", &GeometryTensorQO::tensor_op)
         .def_readwrite("precision", &GeometryTensorQO::precision)
+        .def_readwrite("params_ready", &GeometryTensorQO::params_ready)
         .def_readonly("planes_bf16", &GeometryTensorQO::planes_bf16)
         .def_readonly("lines_bf16", &GeometryTensorQO::lines_bf16)
         .def("RefreshLowPrecision", &GeometryTensorQO::RefreshLowPrecision)

@@ -5,6 +5,7 @@
 // GeometryTensorQO (geometry_tensor_qo.cpp:257-390) and the fused projection
 // with its hand-written adjoint.
 #include <ATen/cuda/CUDAContext.h>
+#include <cuda_runtime_api.h>
 
 #include "atdf_host.h"
 
@@ -578,6 +579,8 @@ struct ProjectArgs {
     Tensor bins;    // uniform samples: also bin rho * w per segment (optional)
     Tensor ws;      // workspace to use (required with placed samples)
     Tensor xt, xw;  // caller-placed samples: t and weight per sample
+    bool segmented = false;  // ws already holds the uniform segments of these rays (atdf_project_segments)
+    Tensor err;              // device error word to use (optional)
 };
 
 class ProjectFn : public torch::autograd::Function<ProjectFn> {
@@ -603,7 +606,7 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
         auto ws = a->ws.defined() ? a->ws : torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
         TORCH_CHECK((size_t)ws.numel() >= bytes, "ProjectRays: workspace too small");
         auto img = torch::empty({dims.back(), R}, o.options());
-        auto err = err_word(o.device());
+        auto err = a->err.defined() ? a->err : err_word(o.device());
         if (placed) {
             check_status(atdf_project_forward_samples(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R,
                                                       a->xt.data_ptr<float>(), a->xw.data_ptr<float>(),
@@ -618,6 +621,11 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
                                                      ws.data_ptr(), (size_t)ws.numel(), err.data_ptr<int32_t>(),
                                                      stream_arg()),
                          "ProjectRays forward (binned)");
+        } else if (a->segmented) {
+            check_status(atdf_project_forward_segmented(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R,
+                                                        a->seed, img.data_ptr<float>(), ws.data_ptr(),
+                                                        (size_t)ws.numel(), err.data_ptr<int32_t>(), stream_arg()),
+                         "ProjectRays forward (segmented)");
         } else {
             check_status(atdf_project_forward(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R, a->M, a->seed,
                                               img.data_ptr<float>(), ws.data_ptr(), (size_t)ws.numel(),
@@ -676,9 +684,35 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
 };
 
 // The forward reads args only while it runs; the backward uses saved data.
+// The current stream waits for the last parameter update (params_ready).
+static void wait_params(const GeometryTensorQO& geo)
+{
+    if (geo.params_ready == 0) return;
+    TORCH_CHECK(cudaStreamWaitEvent(cur_stream(), reinterpret_cast<cudaEvent_t>(geo.params_ready), 0) == cudaSuccess,
+                "waiting for params_ready failed");
+}
+
 static Tensor project_apply(GeometryTensorQO& geo, ProjectArgs& args, const RayList& rays)
 {
     ATDF_CHECK_CUDA(rays.origin);
+    if (geo.params_ready != 0 && !args.ws.defined() && !args.bins.defined()) {
+        // segments first (rays and tree only), then wait for the parameters
+        auto t = args.tree->view();
+        auto o = rays.origin.contiguous(), d = rays.direction.contiguous();
+        const int64_t R = o.size(0), slots = geo.planes[0].size(0);
+        size_t bytes = 0;
+        check_status(atdf_project_workspace_size(R, t.max_depth, t.ns, slots, 1, &bytes),
+                     "atdf_project_workspace_size");
+        args.ws = torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
+        args.err = err_word(o.device());
+        atdf_segments_t view;
+        check_status(atdf_project_segments(&t, o.data_ptr<float>(), d.data_ptr<float>(), R, args.M, slots,
+                                           args.ws.data_ptr(), bytes, &view, args.err.data_ptr<int32_t>(),
+                                           stream_arg()),
+                     "ProjectRays segments");
+        args.segmented = true;
+    }
+    wait_params(geo);
     std::vector<Tensor> P, L;
     for (int m = 0; m < 3; ++m) {
         P.push_back(channels_last(geo.planes[m]));
@@ -701,6 +735,7 @@ std::tuple<Tensor, Tensor, Tensor> GeometryTensorQO::ProjectNodeError(HyperTreeB
 {
     torch::NoGradGuard ng;
     ATDF_CHECK_CUDA(rays.origin);
+    wait_params(*this);
     std::vector<Tensor> P, L;
     for (int m = 0; m < 3; ++m) {
         P.push_back(channels_last(planes[m]));

@@ -28,16 +28,40 @@ def _dense(t):
 
 
 class Adam(torch.optim.Optimizer):
-    """torch.optim.Adam's update on CUDA FP32 parameters, one fused kernel per
-    parameter. ``geometry``: a GeometryTensorQO whose BF16 working copies
+    """torch.optim.Adam's update on CUDA FP32 parameters, every parameter in
+    one launch. ``geometry``: a GeometryTensorQO whose BF16 working copies
     (planes_bf16 / lines_bf16, precision "bf16") are written in the same pass
-    for its planes and lines; other parameters are updated alone."""
+    for its planes and lines; other parameters are updated alone.
 
-    def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, weight_decay=0.0, geometry=None):
+    ``stream``: run the update on this stream instead of the current one. The
+    step waits for the current stream (the gradients), and an event recorded
+    after it becomes ``geometry.params_ready``. The geometry's projections
+    wait for that event only after their segment pass, which reads only the
+    rays and the tree, so the next step's segment pass overlaps the update.
+    Any other reader of the parameters must call ``wait()`` first."""
+
+    def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, weight_decay=0.0, geometry=None,
+                 stream=None):
         if not 0.0 <= betas[0] < 1.0 or not 0.0 <= betas[1] < 1.0 or eps < 0.0:
             raise ValueError("invalid Adam hyper-parameters")
         super().__init__(params, dict(lr=lr, betas=betas, eps=eps, weight_decay=weight_decay))
         self.geometry = geometry
+        self.stream = stream
+        self._done = None  # event recorded after the last update on `stream`
+
+    def wait(self):
+        """Make the current stream wait for the last update."""
+        if self._done is not None:
+            torch.cuda.current_stream().wait_event(self._done)
+
+    def __del__(self):
+        # the geometry must not keep the handle of an event destroyed with us
+        try:
+            if self._done is not None and self.geometry is not None and \
+                    self.geometry.params_ready == self._done.cuda_event:
+                self.geometry.params_ready = 0
+        except Exception:
+            pass
 
     def _twins(self):
         g = self.geometry
@@ -59,7 +83,8 @@ class Adam(torch.optim.Optimizer):
             with torch.enable_grad():
                 loss = closure()
         L = capi.lib()
-        stream = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+        side = self.stream
+        stream = ct.c_void_p((side or torch.cuda.current_stream()).cuda_stream)
         twins = self._twins()
         batch, keep, copies = [], [], []  # one atdf_adam_step_multi call for every parameter
         for group in self.param_groups:
@@ -95,11 +120,24 @@ class Adam(torch.optim.Optimizer):
                 keep.append(g)
                 if twin is not None and not fused_twin:
                     copies.append((twin, p))
+        if side is not None:  # the gradients, new optimizer state and layout copies come from the current stream
+            side.wait_stream(torch.cuda.current_stream())
         if batch:
             arr = (capi.AdamTensor * len(batch))(*batch)
             status = L.atdf_adam_step_multi(len(batch), arr, stream)
             if status != 0:
                 raise RuntimeError(f"atdf_adam_step_multi: {L.atdf_status_string(status).decode()}")
-        for twin, p in copies:
-            twin.copy_(p)
+        if side is not None:
+            with torch.cuda.stream(side):
+                for twin, p in copies:
+                    twin.copy_(p)
+            for g in keep:  # freed on the current stream while the update may still read them
+                g.record_stream(side)
+            self._done = torch.cuda.Event()
+            self._done.record(side)
+            if self.geometry is not None:
+                self.geometry.params_ready = self._done.cuda_event
+        else:
+            for twin, p in copies:
+                twin.copy_(p)
         return loss

@@ -367,11 +367,13 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
         if geo.precision == "bf16":  # the step also writes the BF16 working copies
             from .optim import Adam
 
-            a = Adam(groups, geometry=geo)
+            # on a side stream: the next step's segment pass overlaps the update
+            a = Adam(groups, geometry=geo, stream=adam_stream)
         else:
             a = torch.optim.Adam(groups, fused=True)
         return a, torch.optim.lr_scheduler.ExponentialLR(a, opt.lr_decay)
 
+    adam_stream = torch.cuda.Stream(device=device)
     adam, sched = make_optimizer(opt.lr_grid, opt.lr_decoder)
     tm = None
     if opt.tone_mapper:
@@ -416,11 +418,26 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
             reached = t_train
         return p
 
-    torch.cuda.synchronize()
+    # The training clock runs from one synchronisation point to the next
+    # (evaluations, the time limit, refinement logs): steps are enqueued back
+    # to back, as in a plain training loop, and evaluation time is excluded.
+    clock = [0.0]
+
+    def pause():
+        nonlocal t_train
+        torch.cuda.synchronize()
+        t_train += time.perf_counter() - clock[0]
+
+    def resume():
+        torch.cuda.synchronize()
+        clock[0] = time.perf_counter()
+
+    if tm is not None:
+        tm.check_errors = False  # image ids come from the series: no per-step read-back
+    resume()
     for epoch in range(opt.epochs):
         perm = torch.randperm(n, device=device, generator=gen)
         for s in range(steps_per_epoch):
-            t0 = time.perf_counter()
             idx = perm[s * opt.batch:(s + 1) * opt.batch]
             rays = RayList(data.origin[idx], data.direction[idx])
             target = data.target[idx]
@@ -448,30 +465,35 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
                         o.zero_grad(set_to_none=True)
                 tm.ApplyConstraints()
             loss_acc += loss.detach().double()
-            torch.cuda.synchronize()
-            t_train += time.perf_counter() - t0
             step += 1
             if opt.eval_every and step % opt.eval_every == 0:
+                pause()
                 evaluate(epoch)
                 if reached is not None and opt.stop_at_target:
                     return records, reached
-            if opt.time_limit and t_train >= opt.time_limit:
+                resume()
+            if opt.time_limit and t_train + (time.perf_counter() - clock[0]) >= opt.time_limit:
+                pause()
                 evaluate(epoch)
                 return records, reached
         sched.step()
         if opt.refine_every and (epoch + 1) % opt.refine_every == 0 and epoch + 1 < opt.epochs:
-            t0 = time.perf_counter()
+            if hasattr(adam, "wait"):
+                adam.wait()
             if refine(tree, geo, data, opt.max_active_nodes or tree.NumActiveNodes(), opt.max_samples_per_node):
                 # reset_optimizer_after_structure_change: fresh Adam state at the current rates
                 adam, sched = make_optimizer(*[g["lr"] for g in adam.param_groups])
-            torch.cuda.synchronize()
-            t_train += time.perf_counter() - t0
             if log:
+                pause()
                 log({"form": form, "refined_epoch": epoch, "leaves": int(tree.NumActiveNodes()), "t": t_train})
+                resume()
         if not opt.eval_every:
+            pause()
             evaluate(epoch)
             if reached is not None and opt.stop_at_target:
                 return records, reached
+            resume()
+    pause()
     return records, reached
 
 

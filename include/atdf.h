@@ -267,6 +267,18 @@ int atdf_project_forward(const atdf_tree_t* tree, const atdf_field_t* field, con
                          int32_t max_samples_per_node, uint64_t jitter_seed, float* image, void* workspace,
                          size_t workspace_bytes, int32_t* dev_error, atdf_stream_t stream);
 
+/* atdf_project_forward in two calls: atdf_project_segments (below) first
+ * writes the ray/leaf segments and their uniform sample counts into the
+ * workspace, then this call projects them. The segment pass reads only the
+ * rays and the tree, so a caller can run it while the factors are still
+ * being updated (an optimizer step on another stream) and make the stream
+ * wait for that update between the two calls. The results equal
+ * atdf_project_forward's. */
+int atdf_project_forward_segmented(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
+                                   const float* ray_origin, const float* ray_direction, int64_t num_rays,
+                                   uint64_t jitter_seed, float* image, void* workspace, size_t workspace_bytes,
+                                   int32_t* dev_error, atdf_stream_t stream);
+
 /* Hand-written adjoint of atdf_project_forward given grad_image [Cout, R]:
  * OVERWRITES grad_field (FP32, channels-last) and grad_mlp. Recomputes every
  * sample (no stored activations); reuses the forward's segments from the

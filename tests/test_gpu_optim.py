@@ -131,3 +131,54 @@ def test_single_tensor_entry_equals_the_batched_launch():
             assert torch.equal(x, y)
     for q, q2 in zip(pb, pb2):
         assert torch.equal(q, q2)
+
+
+def test_update_on_a_side_stream_matches_the_plain_step():
+    """Adam(stream=side) with the geometry's params_ready event: the next
+    projection runs its segment pass (atdf_project_segments), then waits for
+    the update, then projects the segments (atdf_project_forward_segmented).
+    Three training steps give the parameters of the same steps with the
+    update on the current stream. The backward's line and decoder gradients
+    are FP32 atomic sums, so two runs differ in the last bits, and Adam turns
+    a last-bit change of a near-zero gradient into a step of up to 2 lr:
+    two runs of the same path differ by about 1e-4 relative. A projection
+    that read the parameters before their update would differ by about lr in
+    every element (about 2e-2 relative here)."""
+    import gc
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import optim
+    from adaptivetensordf_b200 import synthetic as syn
+
+    tree = syn.make_tree(3, device="cuda")
+    rng = torch.Generator(device="cpu").manual_seed(5)
+    R = 2048
+    o = (torch.rand(R, 3, generator=rng) * 2 - 1) * 0.5
+    d = torch.nn.functional.normalize(torch.randn(R, 3, generator=rng), dim=1)
+    o = (o - 1.7 * d).cuda()
+    d = d.cuda()
+    y = torch.rand(1, R, generator=rng).cuda()
+    runs = []
+    for side in (None, torch.cuda.Stream()):
+        geo = syn.make_geometry(tree, 16, 17, (128, 17, 128), [64, 64], seed=9)
+        geo.precision = "bf16"
+        geo.RefreshLowPrecision()
+        params = syn.parameters(geo)
+        opt = optim.Adam(params, lr=1e-2, geometry=geo, stream=side)
+        for k in range(3):
+            img = geo.ProjectRays(tree, ab.RayList(o, d), 16, 1 + k)
+            loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
+            img.backward(gimg)
+            opt.step()
+            opt.zero_grad(set_to_none=True)
+        if side is not None:
+            assert geo.params_ready != 0
+            opt.wait()
+        torch.cuda.synchronize()
+        runs.append(([p.detach().clone() for p in params], [b.clone() for b in geo.planes_bf16]))
+        del opt
+        gc.collect()
+        assert geo.params_ready == 0  # the optimizer takes its event handle back
+    for a, b in zip(runs[0][0] + runs[0][1], runs[1][0] + runs[1][1]):
+        a, b = a.float(), b.float()
+        assert float((a - b).norm() / a.norm().clamp_min(1e-30)) < 2e-3
