@@ -48,6 +48,7 @@ class Adam(torch.optim.Optimizer):
         self.geometry = geometry
         self.stream = stream
         self._done = None  # event recorded after the last update on `stream`
+        self._inputs = None  # the last update's gradients, held until the current stream has waited for it
 
     def wait(self):
         """Make the current stream wait for the last update."""
@@ -84,6 +85,11 @@ class Adam(torch.optim.Optimizer):
                 loss = closure()
         L = capi.lib()
         side = self.stream
+        if side is not None and self._inputs is not None:
+            # the previous update's gradients may be freed now: the current
+            # stream waits for that update (a projection has usually done so)
+            self.wait()
+            self._inputs = None
         stream = ct.c_void_p((side or torch.cuda.current_stream()).cuda_stream)
         twins = self._twins()
         batch, keep, copies = [], [], []  # one atdf_adam_step_multi call for every parameter
@@ -131,8 +137,11 @@ class Adam(torch.optim.Optimizer):
             with torch.cuda.stream(side):
                 for twin, p in copies:
                     twin.copy_(p)
-            for g in keep:  # freed on the current stream while the update may still read them
-                g.record_stream(side)
+            # the gradients stay referenced until the next step, after the
+            # current stream has waited for this update, so their memory is
+            # reused in stream order (no cross-stream frees, no pool growth
+            # when the host runs ahead of the device)
+            self._inputs = keep
             self._done = torch.cuda.Event()
             self._done.record(side)
             if self.geometry is not None:
