@@ -358,36 +358,58 @@ __device__ __forceinline__ float alloc_weight(const float* lg, float len, float 
     return power == 0.0f ? len : len * __powf(fmaxf(dens, 1e-20f), power);
 }
 
-// One thread per ray: sample counts of the ray's segments from the predicted
-// densities; writes nsamp, first (within the ray) and the ray's total into
+// One warp per ray, a lane per segment (in chunks of 32): sample counts of
+// the ray's segments from the predicted densities; writes nsamp, first
+// (within the ray, a warp scan) and the ray's total into
 // ray_sample_offset[r] (scanned afterwards).
 __global__ void proposal_allocate_kernel(atdf_segments_t segs, int64_t R, const float* __restrict__ logits,
                                          int32_t budget, float mass_mix, float mass_power)
 {
-    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= R) return;
-    const int64_t b = segs.ray_seg_offset[r], e = segs.ray_seg_offset[r + 1];
-    const int nseg = (int)(e - b);
-    float msum = 0.0f, lsum = 0.0f;
-    for (int64_t s = b; s < e; ++s) {
-        const float len = segs.tmax[s] - segs.tmin[s];
-        msum += alloc_weight(logits + s * kPropOut, len, mass_power);
-        lsum += len;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < R; r += warps) {
+        const int64_t b = segs.ray_seg_offset[r], e = segs.ray_seg_offset[r + 1];
+        const int nseg = (int)(e - b);
+        float msum = 0.0f, lsum = 0.0f;
+        for (int64_t s = b + lane; s < e; s += 32) {
+            const float len = segs.tmax[s] - segs.tmin[s];
+            msum += alloc_weight(logits + s * kPropOut, len, mass_power);
+            lsum += len;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            msum += __shfl_xor_sync(0xffffffffu, msum, o);
+            lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        }
+        const int spare = budget > nseg ? budget - nseg : 0;
+        int run = 0;
+        for (int64_t s0 = b; s0 < e; s0 += 32) {
+            const int64_t s = s0 + lane;
+            int n = 0;
+            if (s < e) {
+                const float len = segs.tmax[s] - segs.tmin[s];
+                const float m = alloc_weight(logits + s * kPropOut, len, mass_power);
+                float share = lsum > 0.0f ? len / lsum : 1.0f / (float)nseg;
+                if (msum > 0.0f) share = (1.0f - mass_mix) * (m / msum) + mass_mix * share;
+                n = 1 + (int)floorf((float)spare * share + 0.5f);
+            }
+            int incl = n;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (s < e) {
+                segs.nsamp[s] = n;
+                segs.first[s] = run + incl - n;
+            }
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) {
+            segs.ray_sample_offset[r] = run;
+            atomicMax((unsigned long long*)&segs.totals[2], (unsigned long long)run);
+        }
     }
-    const int spare = budget > nseg ? budget - nseg : 0;
-    int run = 0;
-    for (int64_t s = b; s < e; ++s) {
-        const float len = segs.tmax[s] - segs.tmin[s];
-        const float m = alloc_weight(logits + s * kPropOut, len, mass_power);
-        float share = lsum > 0.0f ? len / lsum : 1.0f / (float)nseg;
-        if (msum > 0.0f) share = (1.0f - mass_mix) * (m / msum) + mass_mix * share;
-        const int n = 1 + (int)floorf((float)spare * share + 0.5f);
-        segs.nsamp[s] = n;
-        segs.first[s] = run;
-        run += n;
-    }
-    segs.ray_sample_offset[r] = run;
-    atomicMax((unsigned long long*)&segs.totals[2], (unsigned long long)run);
 }
 
 // Bin probabilities of a segment: softmax of power * (the 32 logits), i.e.
@@ -406,10 +428,20 @@ __device__ __forceinline__ void bin_probs(const float* lg, float bin_mix, float*
     for (int b = 0; b < kPropBins; ++b) p[b] = p[b] * inv + u;
 }
 
-__global__ void proposal_samples_kernel(atdf_segments_t segs, const float* __restrict__ logits, float bin_mix,
-                                        float bin_power, uint64_t seed, float* __restrict__ sample_t,
-                                        float* __restrict__ sample_w, int64_t capacity, int32_t* err)
+// One thread per segment. The bin probabilities live in shared memory, one
+// column per thread (the bin search indexes them by a run-time bin, which in
+// a register array would go to local memory).
+constexpr int kSampThreads = 256;
+
+__global__ void __launch_bounds__(kSampThreads) proposal_samples_kernel(atdf_segments_t segs,
+                                                                        const float* __restrict__ logits,
+                                                                        float bin_mix, float bin_power, uint64_t seed,
+                                                                        float* __restrict__ sample_t,
+                                                                        float* __restrict__ sample_w, int64_t capacity,
+                                                                        int32_t* err)
 {
+    __shared__ float s_p[kPropBins * kSampThreads];
+    float* p = s_p + threadIdx.x;  // bin b at p[b * kSampThreads]
     const int64_t nseg = segs.totals[0];
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += (int64_t)gridDim.x * blockDim.x) {
         const int n = segs.nsamp[s], r = segs.ray[s], node = segs.node[s];
@@ -419,8 +451,12 @@ __global__ void proposal_samples_kernel(atdf_segments_t segs, const float* __res
             set_err(err, ATDF_DEVERR_SAMPLE_CAPACITY);
             continue;
         }
-        float p[kPropBins];
-        bin_probs(logits + s * kPropOut, bin_mix, p, bin_power);
+        {
+            float q[kPropBins];
+            bin_probs(logits + s * kPropOut, bin_mix, q, bin_power);
+#pragma unroll
+            for (int b = 0; b < kPropBins; ++b) p[b * kSampThreads] = q[b];
+        }
         const float t0 = segs.tmin[s], t1 = segs.tmax[s];
         const float binw = (t1 - t0) / (float)kPropBins;
         int bcur = 0;
@@ -429,11 +465,11 @@ __global__ void proposal_samples_kernel(atdf_segments_t segs, const float* __res
         auto place = [&](int j) {
             const float a = seed ? jitter(seed, r, node, j) : 0.5f;
             const float u = ((float)j + a) / (float)n;
-            while (bcur < kPropBins - 1 && cdf + p[bcur] <= u) {
-                cdf += p[bcur];
+            while (bcur < kPropBins - 1 && cdf + p[bcur * kSampThreads] <= u) {
+                cdf += p[bcur * kSampThreads];
                 ++bcur;
             }
-            float frac = (u - cdf) / p[bcur];
+            float frac = (u - cdf) / p[bcur * kSampThreads];
             frac = fminf(fmaxf(frac, 0.0f), 1.0f);
             const float t = t0 + ((float)bcur + frac) * binw;
             return fminf(fmaxf(t, t0), t1);
@@ -645,8 +681,8 @@ int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, co
     cudaStream_t s = (cudaStream_t)stream;
     ATDF_CUDA_TRY(cudaMemsetAsync(&segments->totals[2], 0, sizeof(int64_t), s));
     if (num_rays > 0) {
-        proposal_allocate_kernel<<<(unsigned)div_up(num_rays, 128), 128, 0, s>>>(*segments, num_rays, logits, budget,
-                                                                                mass_mix, mass_power);
+        const unsigned blocks = (unsigned)std::min<int64_t>(div_up(num_rays, 8), 148 * 16);  // 8 rays per block
+        proposal_allocate_kernel<<<blocks, 256, 0, s>>>(*segments, num_rays, logits, budget, mass_mix, mass_power);
         ATDF_LAUNCH_CHECK();
     }
     ATDF_CUDA_TRY(cudaMemsetAsync(&segments->ray_sample_offset[num_rays], 0, sizeof(int64_t), s));
@@ -664,7 +700,7 @@ int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, 
     if (!segments || !logits || !sample_t || !sample_w || sample_capacity < 0 ||
         !(bin_mix > 0.0f && bin_mix <= 1.0f) || !(bin_power >= 0.0f && bin_power <= 1.0f))
         return ATDF_ERR_INVALID_ARGUMENT;
-    proposal_samples_kernel<<<seg_blocks(segments->capacity), 256, 0, (cudaStream_t)stream>>>(
+    proposal_samples_kernel<<<seg_blocks(segments->capacity), kSampThreads, 0, (cudaStream_t)stream>>>(
         *segments, logits, bin_mix, bin_power, seed, sample_t, sample_w, sample_capacity, dev_error);
     ATDF_LAUNCH_CHECK();
     return ATDF_OK;
