@@ -67,6 +67,35 @@ __global__ void bucket_scatter_kernel(Ws w, atdf_field_t f, int64_t num_nodes)
     }
 }
 
+// Order of the slot queue: slots by descending segment count, so that the
+// largest slots start first and the kernels' tail holds the smallest ones
+// (longest-processing-time-first scheduling of the slot-sticky work). A
+// counting sort on min(segments / 2, 255) in one block; it writes into
+// slot_cursor, whose bucketing role has ended.
+__global__ void slot_order_kernel(Ws w)
+{
+    __shared__ int hist[256];
+    const int n = (int)w.nslot + 1;
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < n; s += blockDim.x)
+        atomicAdd(&hist[255 - min((w.slot_offset[s + 1] - w.slot_offset[s]) >> 1, 255)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int i = 0; i < 256; ++i) {
+            const int c = hist[i];
+            hist[i] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        const int pos = atomicAdd(&hist[255 - min((w.slot_offset[s + 1] - w.slot_offset[s]) >> 1, 255)], 1);
+        w.slot_cursor[pos] = s;
+    }
+}
+
 __global__ void item_count_kernel(Ws w)
 {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s <= w.nslot + 1;
@@ -939,6 +968,8 @@ static int project_forward(const atdf_tree_t* tree, const atdf_field_t* field, c
     bucket_scatter_kernel<<<592, 256, 0, s>>>(w, *field, tree->num_nodes);
     ATDF_LAUNCH_CHECK();
     item_count_kernel<<<(unsigned)div_up(w.nslot + 2, 256), 256, 0, s>>>(w);
+    ATDF_LAUNCH_CHECK();
+    slot_order_kernel<<<1, 1024, 0, s>>>(w);
     ATDF_LAUNCH_CHECK();
     scan_exclusive_i32_kernel<<<1, 1024, 0, s>>>(w.item_offset, w.nslot + 2, nullptr);
     ATDF_LAUNCH_CHECK();

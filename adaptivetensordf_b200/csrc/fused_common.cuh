@@ -32,7 +32,7 @@ struct Ws {
     float* seg_partial;
     int32_t* bucket;
     int32_t* slot_offset;  // [nslot + 2]
-    int32_t* slot_cursor;  // [nslot + 1]
+    int32_t* slot_cursor;  // [nslot + 1]: bucket cursors, then the queue's slot order
     int32_t* item_offset;  // [nslot + 2]
     int32_t* counters;     // [8]
     int64_t cap;
@@ -287,8 +287,9 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
                 const int nslots = (int)w.nslot + 1;  // plane slots + the out-of-ROI bucket
                 s_ctl[4] = -1;
                 while (true) {
-                    const int sl = atomicAdd(&w.counters[queue], 1);
-                    if (sl >= nslots) break;
+                    const int q = atomicAdd(&w.counters[queue], 1);
+                    if (q >= nslots) break;
+                    const int sl = w.slot_cursor[q];  // largest slots first (slot_order_kernel)
                     const int i0 = w.item_offset[sl], i1 = w.item_offset[sl + 1];
                     if (i1 > i0) {
                         s_ctl[4] = sl;
