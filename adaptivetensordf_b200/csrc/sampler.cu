@@ -27,7 +27,7 @@ __device__ __forceinline__ void block_scan_exclusive(T* data, int64_t n, T* tota
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t per = div_up(n, 1024);
     const int64_t b = min(n, (int64_t)tid * per), e = min(n, b + per);
-    constexpr int KEEP = 16;
+    constexpr int KEEP = 17;  // 16384 rays + 1 offsets per 1024 threads
     T keep[KEEP];
     T s = 0;
     if (per <= KEEP) {
