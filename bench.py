@@ -435,8 +435,9 @@ def run_ours(args, rank, world):
     if rank != 0:
         return
     # this library's kernels per uniform training step of the BF16 form: 13 for
-    # sampling, bucketing, projection and loss, and one Adam launch for the 12 parameters
-    launches_per_step = 14
+    # sampling, bucketing (with the slot order), projection and loss, and one
+    # Adam launch for the 12 parameters
+    launches_per_step = 15
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
     # tcgen05 backward launch on this workload at 16384 rays, from a
     # single-pass ncu capture of the bench's warm-up step; the gradient
