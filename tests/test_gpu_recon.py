@@ -100,3 +100,21 @@ def test_training_forms_follow_the_same_curve():
         assert all(r["t"] > 0 for r in recs) and recs[-1]["t"] >= recs[0]["t"]
         out[form] = recs[-1]["psnr"]
     assert abs(out["fp32"] - out["bf16"]) < 0.5, out
+
+
+def test_training_with_the_proposal_in_the_bf16_form():
+    """The BF16 form through the learned proposal (tensor-core proposal MLP,
+    judge passes, the gate) with the side-stream Adam: the loss falls, every
+    step is accounted to a sampler and the PSNR stays finite."""
+    from adaptivetensordf_b200 import recon
+    from adaptivetensordf_b200 import synthetic as syn
+
+    cfg = syn.Config("small", 32, 12, 9, 15.0, 32, 2, 16, 17, [64, 64], 1024, 16)
+    data = recon.make_tilt_series(cfg)
+    opt = recon.TrainOptions(epochs=4, batch=1024, max_samples_per_node=cfg.max_samples_per_node, eval_every=0,
+                             stop_at_target=False, init_scale=0.05, budget=48)
+    recs, _ = recon.train(cfg, "bf16+prop", data, opt)
+    last = recs[-1]
+    assert last["loss"] < recs[0]["loss"] and math.isfinite(last["psnr"])
+    assert last["judge_steps"] + last["proposal_steps"] + last["uniform_steps"] == last["step"]
+    assert last["judge_steps"] >= 20  # the warm-up judges every step
