@@ -1,8 +1,8 @@
 """ctypes view of the C ABI in include/atdf.h (libatdf_b200.so).
 
-This is the binding a caller outside PyTorch would write;
-the tests use it to drive the kernels through the C ABI with raw device
-pointers. Structures mirror the header field by field.
+This is the binding a caller outside PyTorch would write; the tests use it
+to drive the kernels through the C ABI with raw device pointers. Structures
+mirror the header field by field.
 """
 
 from __future__ import annotations

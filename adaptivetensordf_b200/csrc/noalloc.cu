@@ -14,32 +14,24 @@
 // (counters, bucket counts) on every call, and calls whose work overlaps on
 // the GPU (two streams, or two host threads) race on it.
 
-#include <mutex>
-
 #include "atdf_common.cuh"
 
 static __device__ __align__(256) unsigned char g_project_scratch[ATDF_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of the array on the current device. In host code the name
-// g_project_scratch is only a host-side stand-in, so the address is looked up
-// once per device (with that device current) and cached.
+// Device address of the array in the current device's current context. In
+// host code the name g_project_scratch is only a host-side stand-in, so the
+// address is looked up with that device current. The address belongs to a
+// CUDA context, not to a device ordinal: a caller that runs in a context of
+// its own, or calls again after cudaDeviceReset, gets another one. So it is
+// looked up on every call (a host-side table lookup once the library's
+// module is loaded in the context; the first call in a context loads it) and
+// never cached.
 int scratch_address(void** out)
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return ATDF_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return ATDF_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_project_scratch) != cudaSuccess || !p) return ATDF_ERR_CUDA;
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_project_scratch) != cudaSuccess || !p) return ATDF_ERR_CUDA;
+    *out = p;
     return ATDF_OK;
 }
 }  // namespace

@@ -532,10 +532,14 @@ int atdf_tone_response_loss(int32_t response_params, const float* response, floa
  * the library holds until exit. A problem whose workspace
  * (atdf_project_workspace_size) exceeds it is rejected with
  * ATDF_ERR_WORKSPACE before any launch; at depth 4 that is about 10,000
- * rays per call. The first call on a device looks the array's address up
- * (cudaGetSymbolAddress) and caches it; make that first call before any
- * stream capture. All calls share the array: calls that overlap on the GPU
- * race. Inputs and outputs are the caller's, as in atdf_project_forward. */
+ * rays per call. Every call looks the array's address up in the current
+ * context (cudaGetSymbolAddress, no device work); the first call in a context
+ * loads the library's module there, so make that first call on each device
+ * before any stream capture. All calls share the array: calls that overlap on
+ * the GPU race. Inputs and outputs are the caller's, as in
+ * atdf_project_forward. It is forward only: the segments it leaves in the
+ * array are not a workspace that atdf_project_backward can take, so a caller
+ * that needs gradients uses atdf_project_forward with its own workspace. */
 #define ATDF_NOALLOC_SCRATCH_BYTES (16u << 20)
 int atdf_project_forward_noalloc(const atdf_tree_t* tree, const atdf_field_t* field, const atdf_mlp_t* mlp,
                                  const float* ray_origin, const float* ray_direction, int64_t num_rays,
