@@ -7,9 +7,12 @@ The native pieces live next to this file:
   * _atdf_host*.so    the C++/libtorch host layer with the reference's
                       operator surface (HyperTreeBase, SampleList,
                       IndirectGridSample2D/1D, GeometryTensorQO, ...).
-Both are built in place by ``adaptivetensordf_b200/build.py``. Importing
-this package loads them and fails loudly when they are missing: there is no
-CPU or pure-PyTorch fallback for the path.
+Both are built in place by ``adaptivetensordf_b200/build.py``. The first use
+of a native name (``HyperTreeBase``, ``GeometryTensorQO``, ``ext``, ...) loads
+them and fails loudly when they are missing: there is no CPU or pure-PyTorch
+fallback for the path. The workload generators of ``synthetic`` (numpy
+phantoms, rays, projections and tree refinement) load nothing native until
+they build a tree or a geometry.
 """
 
 from __future__ import annotations
@@ -35,21 +38,20 @@ def _load_ext():
     return _atdf_host
 
 
-ext = _load_ext()
+_NATIVE = ("HyperTreeBase", "RayList", "SampleList", "GeometryTensorQO", "IndirectGridSample2D",
+           "IndirectGridSample1D", "GradientCorrection", "IntegrateSamplesXRay", "AccumulateSampleLossPerNode",
+           "MseLossAndGrad", "DecodeFeatures", "SiddonProject", "ProposalSampler")
+_ext = None
 
-HyperTreeBase = ext.HyperTreeBase
-RayList = ext.RayList
-SampleList = ext.SampleList
-GeometryTensorQO = ext.GeometryTensorQO
-IndirectGridSample2D = ext.IndirectGridSample2D
-IndirectGridSample1D = ext.IndirectGridSample1D
-GradientCorrection = ext.GradientCorrection
-IntegrateSamplesXRay = ext.IntegrateSamplesXRay
-AccumulateSampleLossPerNode = ext.AccumulateSampleLossPerNode
-MseLossAndGrad = ext.MseLossAndGrad
-DecodeFeatures = ext.DecodeFeatures
-SiddonProject = ext.SiddonProject
-ProposalSampler = ext.ProposalSampler
+
+def __getattr__(name):
+    global _ext
+    if name == "ext" or name in _NATIVE:
+        if _ext is None:
+            _ext = _load_ext()
+        return _ext if name == "ext" else getattr(_ext, name)
+    raise AttributeError(f"module 'adaptivetensordf_b200' has no attribute '{name}'")
+
 
 __all__ = [
     "ext",

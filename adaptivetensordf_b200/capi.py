@@ -247,6 +247,46 @@ def field_struct(geo, planes=None, lines=None):
     return f, (planes, lines)
 
 
+def field_struct_bf16(geo):
+    """The field over the geometry's BF16 working copies (RefreshLowPrecision)."""
+    f = Field()
+    planes, lines = list(geo.planes_bf16), list(geo.lines_bf16)
+    f.channels = planes[0].shape[1]
+    f.mode = 1 if geo.tensor_op == "cat" else 0
+    f.dtype = 1
+    for m in range(3):
+        f.plane[m] = planes[m].data_ptr()
+        f.plane_h[m] = planes[m].shape[2]
+        f.plane_w[m] = planes[m].shape[3]
+        f.line[m] = lines[m].data_ptr()
+        f.line_len[m] = lines[m].shape[2]
+        f.roi_min[m] = geo.roi_min[m]
+        f.roi_max[m] = geo.roi_max[m]
+    f.leaf_slot = geo.leaf_slot.data_ptr()
+    f.num_slots = planes[0].shape[0]
+    return f, (planes, lines)
+
+
+def grad_structs(geo, device="cuda"):
+    """Preallocated FP32 gradient buffers shaped like the parameters
+    (channels-last planes / lines) and their C structures."""
+    import torch
+
+    gp = [torch.empty_like(p, memory_format=torch.channels_last) for p in geo.planes]
+    gl = [torch.empty_like(ln, memory_format=torch.channels_last) for ln in geo.lines]
+    gw = [torch.empty_like(w) for w in geo.decoder_weight]
+    gb = [torch.empty_like(b) for b in geo.decoder_bias]
+    fg = FieldGrad()
+    for m in range(3):
+        fg.plane[m] = gp[m].data_ptr()
+        fg.line[m] = gl[m].data_ptr()
+    mg = MlpGrad()
+    for i in range(len(gw)):
+        mg.weight[i] = gw[i].data_ptr()
+        mg.bias[i] = gb[i].data_ptr()
+    return fg, mg, (gp, gl, gw, gb)
+
+
 ACT = {"id": 0, "none": 0, "relu": 1, "silu": 2, "sigmoid": 3, "softplus": 4, "leakyrelu": 5, "abs": 6, "tanh": 7}
 
 

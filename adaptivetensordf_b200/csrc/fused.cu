@@ -50,11 +50,16 @@ constexpr int kSPT = kThreads / kT;   // threads per sample
 // ---------------------------------------------------------------------------
 // bucketing by plane slot
 // ---------------------------------------------------------------------------
-__global__ void bucket_count_kernel(Ws w, atdf_field_t f, int64_t num_nodes)
+// A segment whose node id or plane slot is out of range sets the index bit
+// and joins the out-of-ROI bucket (zero features, no gradient).
+__global__ void bucket_count_kernel(Ws w, atdf_field_t f, int64_t num_nodes, int32_t* err)
 {
     const int64_t nseg = min(w.totals[0], w.cap);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&w.slot_offset[seg_slot(f, num_nodes, w.node[i])], 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t nd = w.node[i];
+        if (nd < 0 || nd >= num_nodes || f.leaf_slot[nd] >= f.num_slots) set_err(err, ATDF_DEVERR_INDEX);
+        atomicAdd(&w.slot_offset[seg_slot(f, num_nodes, nd)], 1);
+    }
 }
 
 __global__ void bucket_scatter_kernel(Ws w, atdf_field_t f, int64_t num_nodes)
@@ -879,17 +884,18 @@ static int prepare(const atdf_tree_t* tree, const atdf_field_t* field, const atd
     }
     for (int l = 0; l < mlp->num_layers; ++l)
         if (!mlp->weight[l] || !mlp->bias[l]) return ATDF_ERR_INVALID_ARGUMENT;
-    // The BF16 tensor-core kernels keep each plane in shared memory with rows
-    // padded to a pitch of 2 mod 4 texels (texel = 16 channels = 32 bytes):
-    // the four corners of a bilinear footprint then have texel indices of
-    // all four residues mod 4 and fill distinct bank groups.
+    // The 16-channel BF16 tensor-core kernels keep each plane in shared
+    // memory with rows padded to a pitch of 2 mod 4 texels (texel = 16
+    // channels = 32 bytes): the four corners of a bilinear footprint then
+    // have texel indices of all four residues mod 4 and fill distinct bank
+    // groups. The 24-channel ones keep the planes unpadded.
     int off = 0, goff = 0;
     for (int m = 0; m < 3; ++m) {
         if (!field->plane[m] || !field->line[m] || ((uintptr_t)field->plane[m] & 15) ||
             ((uintptr_t)field->line[m] & 15))
             return ATDF_ERR_UNSUPPORTED;
         const int W = field->plane_w[m];
-        p.plane_pitch[m] = field->dtype == ATDF_BF16 ? W + ((2 - W) & 3) : W;
+        p.plane_pitch[m] = (field->dtype == ATDF_BF16 && field->channels == 16) ? W + ((2 - W) & 3) : W;
         p.plane_off[m] = off;
         off += field->plane_h[m] * p.plane_pitch[m] * field->channels;
         p.gplane_off[m] = goff;
@@ -961,7 +967,7 @@ static int project_forward(const atdf_tree_t* tree, const atdf_field_t* field, c
     ATDF_CUDA_TRY(cudaMemsetAsync(w.slot_offset, 0, (w.nslot + 2) * 4, s));
     ATDF_CUDA_TRY(cudaMemsetAsync(w.slot_cursor, 0, (w.nslot + 1) * 4, s));
     ATDF_CUDA_TRY(cudaMemsetAsync(w.counters, 0, 8 * 4, s));
-    bucket_count_kernel<<<592, 256, 0, s>>>(w, *field, tree->num_nodes);
+    bucket_count_kernel<<<592, 256, 0, s>>>(w, *field, tree->num_nodes, dev_error);
     ATDF_LAUNCH_CHECK();
     scan_exclusive_i32_kernel<<<1, 1024, 0, s>>>(w.slot_offset, w.nslot + 2, nullptr);
     ATDF_LAUNCH_CHECK();

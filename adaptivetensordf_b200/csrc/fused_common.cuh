@@ -541,9 +541,13 @@ __device__ __forceinline__ void add_to_bins(const FusedParams& p, const SegTab& 
     atomicAdd(&p.bins[(int64_t)tab.id[si] * kBins + b], v);
 }
 
-// BF16 tensor-core variant (fused_tc.cu).
+// BF16 tensor-core variants: 16 channels (fused_tc.cu) and 24 channels
+// (fused_tc24.cu); launch_tc_* dispatch on the field's channel count.
 bool tc_supported(const atdf_field_t* f, const atdf_mlp_t* m);
+bool tc24_supported(const atdf_field_t* f, const atdf_mlp_t* m);
 int launch_tc_forward(const FusedParams& p, cudaStream_t st);
 int launch_tc_backward(const FusedParams& p, cudaStream_t st);
+int launch_tc24_forward(const FusedParams& p, cudaStream_t st);
+int launch_tc24_backward(const FusedParams& p, cudaStream_t st);
 
 }  // namespace atdf

@@ -142,10 +142,12 @@ __global__ void gradcorr_bwd_kernel(const float* __restrict__ dir, const int64_t
     }
     const float d0 = dir[3 * r], d1 = dir[3 * r + 1], d2 = dir[3 * r + 2];
     const float g0 = gin[3 * i], g1 = gin[3 * i + 1], g2 = gin[3 * i + 2];
-    const float dot = g0 * d0 + g1 * d1 + g2 * d2;
-    gout[3 * i] = g0 - dot * d0;
-    gout[3 * i + 1] = g1 - dot * d1;
-    gout[3 * i + 2] = g2 - dot * d2;
+    // grad - grad.dot(direction) * direction, one rounding per operation
+    // (the dot product summed left to right), so the result is reproducible
+    const float dot = __fadd_rn(__fadd_rn(__fmul_rn(g0, d0), __fmul_rn(g1, d1)), __fmul_rn(g2, d2));
+    gout[3 * i] = __fsub_rn(g0, __fmul_rn(dot, d0));
+    gout[3 * i + 1] = __fsub_rn(g1, __fmul_rn(dot, d1));
+    gout[3 * i + 2] = __fsub_rn(g2, __fmul_rn(dot, d2));
 }
 
 // ---------------------------------------------------------------------------

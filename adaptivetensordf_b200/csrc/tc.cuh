@@ -104,6 +104,19 @@ __device__ __forceinline__ void ld_32x32b_x4(uint32_t taddr, uint32_t (&r)[4])
                  : "r"(taddr));
 }
 
+// 32 lanes x 2 columns of 32 bits, raw words.
+__device__ __forceinline__ void ld_32x32b_x2(uint32_t taddr, uint32_t (&r)[2])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
+}
+
+// Thread i of the warp stores 2 words to lane (base + i), columns col..col+1.
+__device__ __forceinline__ void st_32x32b_x2(uint32_t taddr, const uint32_t (&r)[2])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};" ::"r"(taddr), "r"(r[0]), "r"(r[1])
+                 : "memory");
+}
+
 // Thread i of the warp stores 4 words to lane (base + i), columns col..col+3.
 __device__ __forceinline__ void st_32x32b_x4(uint32_t taddr, const uint32_t (&r)[4])
 {

@@ -125,6 +125,14 @@ struct GeometryTensorQO {
     // read the parameters, before the current stream waits for the event.
     int64_t params_ready = 0;
     void RefreshLowPrecision();
+    // Device error word of the fused projection (ProjectRays), accumulated
+    // over calls so that the hot path never reads it back. CheckErrors()
+    // reads it (one synchronisation), clears it and raises if a kernel set a
+    // bit (an index out of range, a capacity exceeded); a training loop calls
+    // it where it synchronises anyway (an evaluation).
+    torch::Tensor fused_error;
+    torch::Tensor error_word(const torch::Device& dev);
+    void CheckErrors();
 
     atdf_field_t view() const;
     torch::Tensor SampleVolumeIndirect_feature(HyperTreeBase& tree, torch::Tensor global_coordinate,

@@ -106,6 +106,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def_readonly("planes_bf16", &GeometryTensorQO::planes_bf16)
         .def_readonly("lines_bf16", &GeometryTensorQO::lines_bf16)
         .def("RefreshLowPrecision", &GeometryTensorQO::RefreshLowPrecision)
+        .def("CheckErrors", &GeometryTensorQO::CheckErrors)
         .def_property(
             "decoder_weight", [](GeometryTensorQO& g) { return g.decoder.weight; },
             [](GeometryTensorQO& g, std::vector<torch::Tensor> v) { g.decoder.weight = v; })

@@ -63,6 +63,9 @@ class GridSample2DFn : public torch::autograd::Function<GridSample2DFn> {
                                                 idx.data_ptr<int64_t>(), u.data_ptr<float>(), S, out.data_ptr<float>(),
                                                 err.data_ptr<int32_t>(), stream_arg()),
                      "IndirectGridSample2D");
+        // data-dependent problems (an index out of range) raise here, as the
+        // reference checks for errors after every op (CUDA_SYNC_CHECK_ERROR)
+        check_dev_error(err, "IndirectGridSample2D");
         ctx->save_for_backward({grid, idx, u});
         ctx->saved_data["err"] = err;
         return out;
@@ -81,6 +84,7 @@ class GridSample2DFn : public torch::autograd::Function<GridSample2DFn> {
                                                  idx.size(0), g.data_ptr<float>(), ggrid.data_ptr<float>(),
                                                  guv.data_ptr<float>(), err.data_ptr<int32_t>(), stream_arg()),
                      "IndirectGridSample2D backward");
+        check_dev_error(err, "IndirectGridSample2D backward");
         return {ggrid, Tensor(), guv};
     }
 };
@@ -105,6 +109,7 @@ class GridSample1DFn : public torch::autograd::Function<GridSample1DFn> {
                                                 idx.data_ptr<int64_t>(), u.data_ptr<float>(), S, out.data_ptr<float>(),
                                                 err.data_ptr<int32_t>(), stream_arg()),
                      "IndirectGridSample1D");
+        check_dev_error(err, "IndirectGridSample1D");
         ctx->save_for_backward({grid, idx, u});
         ctx->saved_data["err"] = err;
         return out;
@@ -123,6 +128,7 @@ class GridSample1DFn : public torch::autograd::Function<GridSample1DFn> {
                                                  g.data_ptr<float>(), ggrid.data_ptr<float>(), guv.data_ptr<float>(),
                                                  err.data_ptr<int32_t>(), stream_arg()),
                      "IndirectGridSample1D backward");
+        check_dev_error(err, "IndirectGridSample1D backward");
         return {ggrid, Tensor(), guv};
     }
 };
@@ -156,6 +162,7 @@ class GradCorrFn : public torch::autograd::Function<GradCorrFn> {
                                                        g.data_ptr<float>(), g.size(0), out.data_ptr<float>(),
                                                        err.data_ptr<int32_t>(), stream_arg()),
                      "GradientCorrection backward");
+        check_dev_error(err, "GradientCorrection backward");
         return {out, Tensor(), Tensor()};
     }
 };
@@ -181,6 +188,7 @@ class IntegrateFn : public torch::autograd::Function<IntegrateFn> {
         check_status(atdf_integrate_xray(v.data_ptr<float>(), w.data_ptr<float>(), r.data_ptr<int64_t>(), v.size(0),
                                          (int32_t)C, R, img.data_ptr<float>(), err.data_ptr<int32_t>(), stream_arg()),
                      "IntegrateSamplesXRay");
+        check_dev_error(err, "IntegrateSamplesXRay");
         ctx->save_for_backward({v, w, r});
         ctx->saved_data["vshape"] = values.sizes().vec();
         ctx->saved_data["wshape"] = weight.sizes().vec();
@@ -222,6 +230,7 @@ std::pair<Tensor, Tensor> AccumulateSampleLossPerNode(const SampleList& samples,
                                                w.size(0), num_nodes, ls.data_ptr<double>(), ws.data_ptr<double>(),
                                                err.data_ptr<int32_t>(), stream_arg()),
                  "AccumulateSampleLossPerNode");
+    check_dev_error(err, "AccumulateSampleLossPerNode");
     return {ls, ws};
 }
 
@@ -430,6 +439,20 @@ void GeometryTensorQO::RefreshLowPrecision()
     }
 }
 
+Tensor GeometryTensorQO::error_word(const torch::Device& dev)
+{
+    if (!fused_error.defined() || fused_error.device() != dev) fused_error = err_word(dev);
+    return fused_error;
+}
+
+void GeometryTensorQO::CheckErrors()
+{
+    if (!fused_error.defined()) return;
+    auto e = fused_error.clone();
+    fused_error.zero_();
+    check_dev_error(e, "ProjectRays");
+}
+
 // Field view over the BF16 working copies (the shapes are the FP32 ones).
 static atdf_field_t field_view_bf16(const GeometryTensorQO& g, const std::vector<Tensor>& planes32)
 {
@@ -501,6 +524,7 @@ class VmFeatureFn : public torch::autograd::Function<VmFeatureFn> {
                                               pc.data_ptr<float>(), nc.data_ptr<int64_t>(), S, out.data_ptr<float>(),
                                               err.data_ptr<int32_t>(), stream_arg()),
                      "SampleVolumeIndirect_feature");
+        check_dev_error(err, "SampleVolumeIndirect_feature");
         ctx->save_for_backward({pc, nc, p0, p1, p2, l0, l1, l2});
         ctx->saved_data["geo"] = geo_ptr;
         ctx->saved_data["tree"] = tree_ptr;
@@ -526,6 +550,7 @@ class VmFeatureFn : public torch::autograd::Function<VmFeatureFn> {
                                                s[0].data_ptr<float>(), s[1].data_ptr<int64_t>(), s[1].size(0),
                                                g.data_ptr<float>(), &gv, err.data_ptr<int32_t>(), stream_arg()),
                      "SampleVolumeIndirect_feature backward");
+        check_dev_error(err, "SampleVolumeIndirect_feature backward");
         return {Tensor(), Tensor(), gp[0], gp[1], gp[2], gl[0], gl[1], gl[2], Tensor(), Tensor()};
     }
 };
@@ -606,7 +631,7 @@ class ProjectFn : public torch::autograd::Function<ProjectFn> {
         auto ws = a->ws.defined() ? a->ws : torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
         TORCH_CHECK((size_t)ws.numel() >= bytes, "ProjectRays: workspace too small");
         auto img = torch::empty({dims.back(), R}, o.options());
-        auto err = a->err.defined() ? a->err : err_word(o.device());
+        auto err = a->err.defined() ? a->err : a->geo->error_word(o.device());
         if (placed) {
             check_status(atdf_project_forward_samples(&t, &f, &m, o.data_ptr<float>(), d.data_ptr<float>(), R,
                                                       a->xt.data_ptr<float>(), a->xw.data_ptr<float>(),
@@ -704,7 +729,7 @@ static Tensor project_apply(GeometryTensorQO& geo, ProjectArgs& args, const RayL
         check_status(atdf_project_workspace_size(R, t.max_depth, t.ns, slots, 1, &bytes),
                      "atdf_project_workspace_size");
         args.ws = torch::empty({(int64_t)bytes}, o.options().dtype(torch::kUInt8));
-        args.err = err_word(o.device());
+        args.err = geo.error_word(o.device());
         atdf_segments_t view;
         check_status(atdf_project_segments(&t, o.data_ptr<float>(), d.data_ptr<float>(), R, args.M, slots,
                                            args.ws.data_ptr(), bytes, &view, args.err.data_ptr<int32_t>(),

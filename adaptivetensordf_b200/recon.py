@@ -404,6 +404,7 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
 
     def evaluate(epoch):
         nonlocal reached
+        geo.CheckErrors()  # device error bits of the steps since the last evaluation
         p = psnr(tree, geo, data.volume) if data.volume is not None else None  # no ground truth: loss only
         rec = {"form": form, "t": t_train, "step": step, "epoch": epoch, "psnr": p,
                "loss": float(loss_acc) / max(1, step)}

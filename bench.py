@@ -1,7 +1,13 @@
 """Benchmark of the differentiable forward projection: fwd+bwd rays/s of one
-training step (fused projection, MSE loss, hand-written adjoint, Adam update)
-on the depth-4 octree / rank-16 VM / 16->64->64->1 decoder workload with
-16384-ray batches of a 256^2 x 61-tilt parallel-beam series.
+training step (fused projection, MSE loss, hand-written adjoint, Adam update).
+
+Headline workload (the largest configuration that fits one GPU): the thin
+slab, a 1024 x 1024 x 256 phantom of 5000 ellipsoids tilted off-axis, 81
+tilts on a 1024^2 detector, an adaptive octree refined to depth 6 with about
+4096 active leaves, rank-24 VM in BF16 with the decoder 24 -> 64 -> 64 -> 1 on
+the tensor cores, 16384-ray batches. The depth-4 / rank-16 workload (256^3
+phantom, 61 tilts, 256^2 detector) is measured beside it in the plain FP32
+form and the chosen BF16 form, with the seconds to a PSNR target.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -9,12 +15,13 @@ Prints one JSON line (rank 0). Under torchrun each rank trains on its own ray
 batches and the gradients are all-reduced once per step (ray data
 parallelism; weak scaling). `--impl reference` times the CPU restatement of
 the reference path (the reference itself has no CPU path and cannot be built
-here) on all host cores.
+here) on all host cores, on the headline workload.
 """
 
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -30,12 +37,21 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd rays/s"
-# samples per ray of the learned proposal: the smallest budget whose
-# projection error against the uniform judge stays within the 1% gate on the
-# C2 series (0.9-1.0% at 160, 1.0-1.4% at 128)
+# samples per ray of the learned proposal on the depth-4 workload: the
+# smallest budget whose projection error against the uniform judge stays
+# within the 1% gate on its tilt series (0.9-1.0% at 160, 1.0-1.4% at 128)
 PROPOSAL_BUDGET = 160
-WORKLOAD = "C2: 256^3 phantom (200 ellipsoids), 61 tilts x 256^2 detector, octree depth 4 (4096 leaves), " \
-           "rank-16 VM 17^2 planes, decoder 16->64->64->1, 16384-ray batch, 24 samples/leaf-diagonal"
+
+
+def workload_name(cfg):
+    if cfg.name == "C5":
+        return ("C5: 1024x1024x256 slab phantom (5000 ellipsoids, off-axis tilt "
+                f"{cfg.off_axis_deg:.2f} deg), 81 tilts x 1024^2 detector, adaptive octree to depth 6 "
+                f"(~{cfg.target_leaves} leaves), rank-24 VM 17^2 planes, decoder 24->64->64->1 BF16, "
+                f"{cfg.rays_per_batch}-ray batch, {cfg.max_samples_per_node} samples/leaf-diagonal")
+    return ("C2: 256^3 phantom (200 ellipsoids), 61 tilts x 256^2 detector, octree depth 4 (4096 leaves), "
+            "rank-16 VM 17^2 planes, decoder 16->64->64->1, 16384-ray batch, "
+            f"{cfg.max_samples_per_node} samples/leaf-diagonal")
 
 
 def parse():
@@ -48,6 +64,7 @@ def parse():
     ap.add_argument("--cpu-rays", type=int, default=128, help="rays per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-psnr", action="store_true", help="skip the seconds-to-PSNR runs")
+    ap.add_argument("--no-psnr30", action="store_true", help="skip the seconds-to-30 dB runs")
     ap.add_argument("--psnr-target", type=float, default=18.0)
     ap.add_argument("--psnr-epochs", type=int, default=3)
     return ap.parse_args()
@@ -56,20 +73,23 @@ def parse():
 # ----------------------------------------------------------------------------
 # workload
 # ----------------------------------------------------------------------------
-def workload_config():
+def workload_config(name="C5"):
     from adaptivetensordf_b200.synthetic import CONFIGS
 
-    return CONFIGS["C2"]
+    return CONFIGS[name]
 
 
-def make_batches(cfg, R, nb, seed):
+def make_batches(cfg, R, nb, seed, device=None):
+    """nb batches of R rays of the configuration's tilt series (random tilt
+    and pixel) with the phantom's analytic line integrals as targets
+    (computed on `device` when one is given)."""
     from adaptivetensordf_b200 import synthetic as syn
 
-    ph = syn.ellipsoid_phantom(cfg.ellipsoids, 1001)
+    ph = syn.config_phantom(cfg, 1001)
     out = []
     for b in range(nb):
         o, d = syn.random_ray_batch(cfg, R, seed + b)
-        y = syn.analytic_projection(ph, o, d).astype(np.float32)
+        y = syn.analytic_projection(ph, o, d, device=device).astype(np.float32)
         out.append((o, d, y))
     return out
 
@@ -136,12 +156,42 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 # CPU baseline (the oracle port of the reference path)
 # ----------------------------------------------------------------------------
-def cpu_baseline(cfg, R, steps=1, seed=77):
+def oracle_tree(cfg):
+    """The workload's tree in the oracle's form: every depth-tree_depth node
+    active, or the adaptive leaves of the configuration's phantom."""
     from adaptivetensordf_b200 import synthetic as syn
     from oracle import oracle as O
 
     t = O.tree_build(cfg.tree_depth)
-    O.set_active_depth(t, cfg.tree_depth)
+    if cfg.target_leaves:
+        leaves, _ = syn.adaptive_leaves(cfg, syn.config_phantom(cfg, 1001), t["node_position_min"],
+                                        t["node_position_max"], t["node_children"], t["node_depth"])
+        act = np.zeros(len(t["node_depth"]), np.int32)
+        act[leaves] = 1
+        O.set_active(t, act)
+    else:
+        O.set_active_depth(t, cfg.tree_depth)
+    return t
+
+
+def batch_counts(cfg, t, R):
+    """Segments and uniform samples of the workload's first batch (the
+    config keys both arms report)."""
+    from oracle import oracle as O
+
+    from adaptivetensordf_b200 import synthetic as syn
+
+    o, d = syn.random_ray_batch(cfg, R, 1004)
+    segs = O.ray_segments(t, o, d, cfg.max_samples_per_node)
+    return len(segs["n"]), int(segs["n"].sum())
+
+
+def cpu_baseline(cfg, t, R, steps=1, seed=77):
+    """The oracle's plain FP32 training step (segments, samples, VM field,
+    decoder, integral, MSE loss, hand-written adjoint) on R rays of the
+    workload, all OpenMP threads."""
+    from oracle import oracle as O
+
     N = len(t["active_node_ids"])
     rng = np.random.default_rng(1003)
     C, G = cfg.channels, cfg.grid
@@ -160,24 +210,34 @@ def cpu_baseline(cfg, R, steps=1, seed=77):
         O.train_step(t, field, mlp, o, d, y, cfg.max_samples_per_node, 1234)
         times.append(time.perf_counter() - t0)
     return {"value": R / statistics.median(times), "unit": "rays/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"{R} rays of the workload per step (same tree, field shapes, decoder, M), median of "
-                      f"{len(times)} steps, {O.num_threads()} OpenMP threads"}
+            "sample": f"{R} rays of the {cfg.name} workload per step (same tree, field shapes, decoder, samples "
+                      f"per leaf diagonal), FP32, median of {len(times)} steps, {O.num_threads()} OpenMP threads"}
+
+
+def shared_config(cfg, leaves, nseg, nsamp):
+    """Config keys both arms report for the same workload."""
+    return {"workload": workload_name(cfg), "rays_per_gpu_step": cfg.rays_per_batch, "samples_per_step": nsamp,
+            "segments_per_step": nseg, "leaves": leaves,
+            "l2": "inputs larger than L2 (BF16 factors read and FP32 gradients written per step)"}
 
 
 def run_reference(args, rank, world):
-    cfg = workload_config()
     if rank != 0:
         return
+    cfg = workload_config()
+    t = oracle_tree(cfg)
+    nseg, nsamp = batch_counts(cfg, t, cfg.rays_per_batch)
     R = args.cpu_rays
     for _ in range(max(args.warmup, 0) and 1):
-        cpu_baseline(cfg, R, 1, seed=5)
+        cpu_baseline(cfg, t, R, 1, seed=5)
     t0 = time.perf_counter()
-    cb = cpu_baseline(cfg, R, max(args.steps, 1), seed=9)
+    cb = cpu_baseline(cfg, t, R, max(args.steps, 1), seed=9)
     wall = time.perf_counter() - t0
     line = {"metric": METRIC, "value": cb["value"], "unit": "rays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * R / cb["value"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cpu_rays_per_step": R}, "impl": "reference",
+            "config": shared_config(cfg, len(t["active_node_ids"]), nseg, nsamp),
+            "parallelism": f"CPU, {cb['cores']} OpenMP threads", "cpu_rays_per_step": R, "impl": "reference",
             "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample", "value", "unit")},
             "e2e": {"value": cb["value"], "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
@@ -187,21 +247,11 @@ def run_reference(args, rank, world):
 # ----------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------
-def algorithmic_bytes(cfg, n_slots, R, nseg):
-    F = 3 * cfg.channels * cfg.grid * cfg.grid  # plane elements per leaf
-    plane_bytes = n_slots * F * 4
-    seg_bytes = nseg * 24
-    ray_bytes = R * 32
-    fwd = plane_bytes + seg_bytes + ray_bytes
-    bwd = 2 * plane_bytes + seg_bytes + ray_bytes  # planes read, gradient written
-    return fwd, bwd
-
-
-def measure_proposal(args, tree, cfg, dev_batches, nb, stream):
+def measure_proposal(args, tree, cfg, dev_batches, nb, stream, budget):
     """Steady-state step of the BF16 form through the learned proposal's
-    samples (PROPOSAL_BUDGET per ray; segments, proposal MLP, allocation and
-    sampling included), and the cost of one judge step (uniform binned pass
-    + proposal training), which the schedule runs every 10 steps while the
+    samples (budget per ray; segments, proposal MLP, allocation and sampling
+    included), and the cost of one judge step (uniform binned pass +
+    proposal training), which the schedule runs every 10 steps while the
     proposal is in use."""
     import torch
 
@@ -215,7 +265,7 @@ def measure_proposal(args, tree, cfg, dev_batches, nb, stream):
     params = syn.parameters(geo)
     opt = Adam(params, lr=1e-3, geometry=geo)  # also writes the BF16 working copies
     ps = ab.ProposalSampler(tree.NumNodes(), 64, 3, 1005, "cuda")
-    ps.budget = PROPOSAL_BUDGET
+    ps.budget = budget
     ps.precision = "bf16"  # the proposal MLP on the tensor cores, as in the BF16 form's schedule
     padam = torch.optim.Adam(ps.parameters(), lr=3e-3)
 
@@ -247,16 +297,68 @@ def measure_proposal(args, tree, cfg, dev_batches, nb, stream):
         e1.record(stream)
         torch.cuda.synchronize()
         res[name + "_ms"] = e0.elapsed_time(e1) / args.steps
-    R = args.rays
+    geo.CheckErrors()
+    R = dev_batches[0][0].shape[0]
     amort = (9 * res["proposal_step_ms"] + res["judge_step_ms"]) / 10
-    res.update({"budget_per_ray": PROPOSAL_BUDGET,
+    res.update({"budget_per_ray": budget,
                 "rays_per_s_proposal_steps": R / (res["proposal_step_ms"] * 1e-3),
-                "rays_per_s_with_judge_every_10": R / (amort * 1e-3),
-                "note": "the proposal is used only while its projection error against the uniform judge is "
-                        "<= 1%; on the C2 tilt series the measured error is 0.9-1.0% at 160 samples per ray "
-                        "(1.0-1.4% at 128)"})
+                "rays_per_s_with_judge_every_10": R / (amort * 1e-3)})
     del geo, opt, params, ps
     return res
+
+
+def time_entry_points(tree, geo, o, d, M, seed, reps=10):
+    """GPU time of the fused forward and backward entry points alone, called
+    through the C ABI with preallocated gradients and the forward's
+    workspace (the same segments as a training step), CUDA events on the
+    launching stream. The backward call is the tensor-core backward kernel
+    plus a few memsets; the forward call includes the ray/leaf segment pass
+    and the bucketing before its kernel."""
+    import ctypes as ct
+
+    import torch
+
+    from adaptivetensordf_b200 import capi
+
+    L = capi.lib()
+    st = torch.cuda.current_stream()
+    sp = ct.c_void_p(st.cuda_stream)
+    t = capi.tree_struct(tree)
+    f, keep_f = capi.field_struct_bf16(geo) if geo.precision == "bf16" else capi.field_struct(geo)
+    m, keep_m = capi.mlp_struct(geo)
+    fg, mg, keep_g = capi.grad_structs(geo)
+    R = o.shape[0]
+    size = ct.c_size_t(0)
+    assert L.atdf_project_workspace_size(R, t.max_depth, t.ns, f.num_slots, 1, ct.byref(size)) == 0
+    ws = torch.empty(size.value, dtype=torch.uint8, device="cuda")
+    img = torch.empty(1, R, device="cuda")
+    gimg = torch.full((1, R), 1.0 / R, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def fwd():
+        assert L.atdf_project_forward(ct.byref(t), ct.byref(f), ct.byref(m), capi.ptr(o), capi.ptr(d), R, M, seed,
+                                      capi.ptr(img), capi.ptr(ws), size.value, capi.ptr(err), sp) == 0
+
+    def bwd():
+        assert L.atdf_project_backward(ct.byref(t), ct.byref(f), ct.byref(m), capi.ptr(o), capi.ptr(d), R, M, seed,
+                                       capi.ptr(gimg), ct.byref(fg), ct.byref(mg), capi.ptr(ws), size.value,
+                                       capi.ptr(err), sp) == 0
+
+    out = {}
+    for name, fn in (("forward", fwd), ("backward", bwd)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    assert err.item() == 0, err.item()
+    del keep_f, keep_m, keep_g
+    return out
 
 
 def device_copy_gbs(stream, nbytes=1 << 30, reps=10):
@@ -322,163 +424,265 @@ def time_to_psnr(args):
     return out
 
 
-def run_ours(args, rank, world):
+# the 30 dB workload: the C2 phantom and model on a full-angle, noise-free
+# series (90 tilts at 2 deg, +-89 deg), learning-rate decay 0.99 per epoch,
+# PSNR evaluated every 360 steps, at most 420 s of training per form
+PSNR30 = {"angles": 90, "angle_step": 2.0, "noise": 0.0, "jitter": 0.0, "lr_decay": 0.99, "epochs": 60,
+          "eval_every": 360, "time_limit": 420.0, "proposal_budget": 128, "residual_gate": 0.5}
+
+
+def time_to_psnr30():
+    """Seconds to 30 dB of the plain FP32 form, the BF16 form and the BF16
+    form with the learned proposal, on the 30 dB workload (PSNR30)."""
+    from adaptivetensordf_b200 import recon
+    from adaptivetensordf_b200.synthetic import CONFIGS
+
+    w = PSNR30
+    cfg = dataclasses.replace(CONFIGS["C2"], angles=w["angles"], angle_step=w["angle_step"], noise=w["noise"],
+                              jitter=w["jitter"])
+    data = recon.make_tilt_series(cfg)
+    out = {"target_db": 30.0, "workload": "C2 phantom and model, 90 noise-free tilts at 2 deg (+-89 deg), "
+           "16384-ray batches, lr decay 0.99 per epoch, PSNR every 360 steps", **w}
+    for form in ("fp32", "bf16", "bf16+prop"):
+        opt = recon.TrainOptions(epochs=w["epochs"], batch=cfg.rays_per_batch,
+                                 max_samples_per_node=cfg.max_samples_per_node, eval_every=w["eval_every"],
+                                 target_psnr=30.0, init_scale=0.05, lr_decay=w["lr_decay"],
+                                 time_limit=w["time_limit"], budget=w["proposal_budget"],
+                                 residual_gate=w["residual_gate"])
+        recs, reached = recon.train(cfg, form, data, opt)
+        out[form] = {"seconds": reached, "best_psnr": max(r["psnr"] for r in recs), "steps": recs[-1]["step"],
+                     "train_seconds": recs[-1]["t"]}
+        if form.endswith("+prop"):
+            out[form].update({k: recs[-1][k] for k in ("judge_steps", "proposal_steps", "uniform_steps",
+                                                        "proposal_error")})
+    for form in ("bf16", "bf16+prop"):
+        if out["fp32"]["seconds"] and out[form]["seconds"]:
+            out[f"ratio_fp32_over_{form}"] = out["fp32"]["seconds"] / out[form]["seconds"]
+    del data
+    return out
+
+
+def step_bytes(cfg, n_slots, nseg, R):
+    """Algorithmic bytes of the BF16 backward launch: the BF16 planes read,
+    the FP32 plane gradient written, the segment records and the rays."""
+    F = 3 * cfg.channels * cfg.grid * cfg.grid  # plane elements per leaf
+    return n_slots * F * 2 + n_slots * F * 4 + nseg * 24 + R * 32
+
+
+def measure_form(args, tree, cfg, form, dev_batches, host_batches, world, sampler=None):
+    """One form's training step on a workload: device-timed K steps
+    (inputs resident), the same through the public API with pinned host
+    inputs and the loss read back (e2e), the forward / backward autograd calls
+    and the fused entry points timed alone."""
     import torch
-    import torch.distributed as dist
 
     import adaptivetensordf_b200 as ab
     from adaptivetensordf_b200 import dp
     from adaptivetensordf_b200 import synthetic as syn
     from adaptivetensordf_b200.optim import Adam
 
+    import torch.distributed as dist
+
+    stream = torch.cuda.current_stream()
+    nb = len(dev_batches)
+    M = cfg.max_samples_per_node
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
+    bf16 = form == "bf16"
+    if bf16:
+        geo.precision = "bf16"
+        geo.RefreshLowPrecision()
+    params = syn.parameters(geo)
+    # the BF16 form's Adam also writes the BF16 working copies, on a side
+    # stream so that the next step's segment pass overlaps it; the plain
+    # FP32 form keeps torch's fused Adam
+    opt = Adam(params, lr=1e-3, geometry=geo, stream=torch.cuda.Stream()) if bf16 else \
+        torch.optim.Adam(params, lr=1e-3, fused=True)
+    join = opt.wait if bf16 else (lambda: None)  # the timed region ends after the last update
+
+    def step(o, d, y, k):
+        rays = ab.RayList(o, d)
+        img = geo.ProjectRays(tree, rays, M, 1 + k)
+        loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
+        img.backward(gimg)
+        dp.allreduce_gradients(params, world)
+        opt.step()
+        opt.zero_grad(set_to_none=True)
+        return loss
+
+    for k in range(args.warmup):
+        step(*dev_batches[k % nb], k)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(*dev_batches[k % nb], 100 + k)
+    join()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        dist.barrier()
+    # end to end through the public API with host buffers: H2D of the
+    # batch, D2H of the loss, every step
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    loss_host = torch.zeros(1, dtype=torch.float64).pin_memory()
+
+    def e2e_step(k, base):
+        o, d, y = host_batches[k % nb]
+        og, dg, yg = o.cuda(non_blocking=True), d.cuda(non_blocking=True), y.cuda(non_blocking=True)
+        loss = step(og, dg, yg, base + k)
+        loss_host.copy_(loss.reshape(1), non_blocking=True)
+
+    for k in range(args.warmup):  # the copies' first use of the pinned buffers is not timed
+        e2e_step(k, 300)
+    torch.cuda.synchronize()
+    h0.record(stream)
+    for k in range(args.steps):
+        e2e_step(k, 200)
+    join()
+    h1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = h0.elapsed_time(h1) / args.steps
+    clocks = sampler.stop() if sampler else None
+    # forward and backward autograd calls timed alone (CUDA events on the
+    # launching stream); two more forward passes (no autograd) are queued
+    # between a forward and its backward so the GPU still has work while the
+    # host runs the autograd engine's part of the backward call
+    reps = 5
+    o, d, y = dev_batches[0]
+    rays = ab.RayList(o, d)
+    evs = []
+    for k in range(reps + 1):  # the first repetition warms the allocator up
+        f0, f1, b0, b1 = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        opt.zero_grad(set_to_none=True)
+        f0.record(stream)
+        img = geo.ProjectRays(tree, rays, M, 7)
+        f1.record(stream)
+        gimg = torch.ones_like(img)
+        with torch.no_grad():
+            for _ in range(2):
+                geo.ProjectRays(tree, rays, M, 7)
+        b0.record(stream)
+        img.backward(gimg)
+        b1.record(stream)
+        evs.append((f0, f1, b0, b1))
+    torch.cuda.synchronize()
+    tf = sum(f0.elapsed_time(f1) for f0, f1, _, _ in evs[1:]) / reps
+    tb = sum(b0.elapsed_time(b1) for _, _, b0, b1 in evs[1:]) / reps
+    entry = time_entry_points(tree, geo, o, d, M, 7)
+    geo.CheckErrors()
+    del geo, opt, params
+    torch.cuda.empty_cache()
+    return {"ms": ms, "ms_e2e": ms_e2e, "forward_call_ms": tf, "backward_call_ms": tb,
+            "forward_entry_ms": entry["forward"], "backward_entry_ms": entry["backward"], "clocks": clocks}
+
+
+def prepare_workload(cfg, R, rank, nb=4):
+    import torch
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+
+    if cfg.target_leaves:
+        tree = syn.adaptive_tree(cfg, syn.config_phantom(cfg, 1001), device="cuda")
+    else:
+        tree = syn.make_tree(cfg.tree_depth, device="cuda")
+    batches = make_batches(cfg, R, nb, 1004 + 1000 * rank, device="cuda")
+    # device-resident inputs (value) and pinned host inputs (e2e)
+    dev = [(torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda(), torch.from_numpy(y).cuda()[None])
+           for o, d, y in batches]
+    host = [(torch.from_numpy(o).pin_memory(), torch.from_numpy(d).pin_memory(),
+             torch.from_numpy(y)[None].pin_memory()) for o, d, y in batches]
+    sg = tree.RaySegments(ab.RayList(*dev[0][:2]), cfg.max_samples_per_node)
+    return tree, dev, host, int(sg.num_segments), int(sg.num_samples)
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    cfg = workload_config()
-    R = args.rays
-    M = cfg.max_samples_per_node
-    tree = syn.make_tree(cfg.tree_depth, device="cuda")
-    nb = 4
-    batches = make_batches(cfg, R, nb, 1004 + 1000 * rank)
-    # device-resident inputs (value) and pinned host inputs (e2e)
-    dev_batches = [(torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda(), torch.from_numpy(y).cuda()[None])
-                   for o, d, y in batches]
-    host_batches = [(torch.from_numpy(o).pin_memory(), torch.from_numpy(d).pin_memory(),
-                     torch.from_numpy(y)[None].pin_memory()) for o, d, y in batches]
     stream = torch.cuda.current_stream()
-    n_slots = int(tree.NumActiveNodes())
-    sg = tree.RaySegments(ab.RayList(*dev_batches[0][:2]), M)
+    R = args.rays
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
+    tpeak = peaks.get("bf16_tflops_sustained", 1400.0)
 
-    def measure(form, sampler=None):
-        geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
-        bf16 = form == "bf16"
-        if bf16:
-            geo.precision = "bf16"
-            geo.RefreshLowPrecision()
-        params = syn.parameters(geo)
-        # the BF16 form's Adam also writes the BF16 working copies, on a side
-        # stream so that the next step's segment pass overlaps it; the plain
-        # FP32 form keeps torch's fused Adam
-        opt = Adam(params, lr=1e-3, geometry=geo, stream=torch.cuda.Stream()) if bf16 else \
-            torch.optim.Adam(params, lr=1e-3, fused=True)
-        join = opt.wait if bf16 else (lambda: None)  # the timed region ends after the last update
-
-        def step(o, d, y, k):
-            rays = ab.RayList(o, d)
-            img = geo.ProjectRays(tree, rays, M, 1 + k)
-            loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
-            img.backward(gimg)
-            dp.allreduce_gradients(params, world)
-            opt.step()
-            opt.zero_grad(set_to_none=True)
-            return loss
-
-        for k in range(args.warmup):
-            step(*dev_batches[k % nb], k)
-        torch.cuda.synchronize()
-        if sampler:
-            sampler.start()
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for k in range(args.steps):
-            step(*dev_batches[k % nb], 100 + k)
-        join()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
-        if world > 1:
-            dist.barrier()
-        # end to end through the public API with host buffers: H2D of the
-        # batch, D2H of the loss, every step
-        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        loss_host = torch.zeros(1, dtype=torch.float64).pin_memory()
-
-        def e2e_step(k, base):
-            o, d, y = host_batches[k % nb]
-            og, dg, yg = o.cuda(non_blocking=True), d.cuda(non_blocking=True), y.cuda(non_blocking=True)
-            loss = step(og, dg, yg, base + k)
-            loss_host.copy_(loss.reshape(1), non_blocking=True)
-
-        for k in range(args.warmup):  # the copies' first use of the pinned buffers is not timed
-            e2e_step(k, 300)
-        torch.cuda.synchronize()
-        h0.record(stream)
-        for k in range(args.steps):
-            e2e_step(k, 200)
-        join()
-        h1.record(stream)
-        torch.cuda.synchronize()
-        ms_e2e = h0.elapsed_time(h1) / args.steps
-        clocks = sampler.stop() if sampler else None
-        # forward and backward calls timed alone (CUDA events on the launching
-        # stream). The calls are enqueued back to back with no host
-        # synchronisation in between, and two more forward passes (no autograd)
-        # are queued between a forward and its backward, so the GPU still has
-        # work queued while the host runs the autograd engine's part of the
-        # backward call: each event pair brackets the call's GPU work only.
-        reps = 5
-        o, d, y = dev_batches[0]
-        rays = ab.RayList(o, d)
-        evs = []
-        for k in range(reps + 1):  # the first repetition warms the allocator up
-            f0, f1, b0, b1 = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-            opt.zero_grad(set_to_none=True)
-            f0.record(stream)
-            img = geo.ProjectRays(tree, rays, M, 7)
-            f1.record(stream)
-            gimg = torch.ones_like(img)
-            with torch.no_grad():
-                for _ in range(2):
-                    geo.ProjectRays(tree, rays, M, 7)
-            b0.record(stream)
-            img.backward(gimg)
-            b1.record(stream)
-            evs.append((f0, f1, b0, b1))
-        torch.cuda.synchronize()
-        tf = sum(f0.elapsed_time(f1) for f0, f1, _, _ in evs[1:])
-        tb = sum(b0.elapsed_time(b1) for _, _, b0, b1 in evs[1:])
-        del geo, opt, params
-        return ms, ms_e2e, tf / reps, tb / reps, clocks
-
+    # headline: the C5 slab in the chosen BF16 form
+    cfg = dataclasses.replace(workload_config("C5"), rays_per_batch=R)
+    tree, dev, host, nseg, nsamp = prepare_workload(cfg, R, rank)
+    n_slots = int(tree.NumActiveNodes())
     sampler = ClockSampler(local)
-    ms, ms_e2e, tf, tb, clocks = measure("bf16", sampler)
-    ms32, ms32_e2e, tf32, tb32, _ = measure("fp32")
-    prop = measure_proposal(args, tree, cfg, dev_batches, nb, stream) if world == 1 else None
+    r5 = measure_form(args, tree, cfg, "bf16", dev, host, world, sampler)
+    prop5 = measure_proposal(args, tree, cfg, dev, len(dev), stream, 64) if world == 1 else None
+    del tree, dev, host
+
+    # the depth-4 / rank-16 workload: plain FP32 against the chosen form
+    cfg2 = dataclasses.replace(workload_config("C2"), rays_per_batch=R)
+    tree2, dev2, host2, nseg2, nsamp2 = prepare_workload(cfg2, R, rank)
+    n_slots2 = int(tree2.NumActiveNodes())
+    r2 = measure_form(args, tree2, cfg2, "bf16", dev2, host2, world)
+    r2_32 = measure_form(args, tree2, cfg2, "fp32", dev2, host2, world)
+    prop2 = measure_proposal(args, tree2, cfg2, dev2, len(dev2), stream, PROPOSAL_BUDGET) if world == 1 else None
+    del tree2, dev2, host2
     copy_gbs = device_copy_gbs(stream) if world == 1 else None
     psnr = time_to_psnr(args) if (world == 1 and not args.no_psnr) else None
+    psnr30 = time_to_psnr30() if (world == 1 and not args.no_psnr and not args.no_psnr30) else None
 
-    esz = 2
-    F = 3 * cfg.channels * cfg.grid * cfg.grid
-    seg_bytes = sg.num_segments * 24 + R * 32
-    fwd_b = n_slots * F * esz + seg_bytes
-    bwd_b = n_slots * F * esz + n_slots * F * 4 + seg_bytes  # BF16 planes read, FP32 gradient written
-    dom_ms, dom_bytes, dom_name = (tb, bwd_b, "backward") if tb >= tf else (tf, fwd_b, "forward")
-    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    h2d = sum(t.numel() * t.element_size() for t in host_batches[0])
-
-    vals = torch.tensor([ms, ms_e2e, ms32], dtype=torch.float64, device="cuda")
+    vals = torch.tensor([r5["ms"], r5["ms_e2e"], r2["ms"], r2_32["ms"]], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, ms_e2e, ms32 = vals.tolist()
+    ms, ms_e2e, ms2, ms2_32 = vals.tolist()
     if rank != 0:
         return
+
+    def rooflines(cfg_, slots, nseg_, nsamp_, r):
+        """The dominant kernel (the BF16 backward, its entry point timed
+        alone) against the HBM and the tensor-core peaks."""
+        kms = r["backward_entry_ms"]
+        assert kms <= r["ms"], (kms, r["ms"])  # a kernel of the step cannot outlast the step
+        nbytes = step_bytes(cfg_, slots, nseg_, R)
+        achieved = nbytes / (kms * 1e-3) / 1e9
+        dims = [cfg_.channels] + list(cfg_.hidden) + [1]
+        flop_fwd = 2 * sum(a * b for a, b in zip(dims[:-1], dims[1:]))  # decoder FLOP per sample, forward
+        flop = 3 * flop_fwd * nsamp_  # recomputed forward + backward (two GEMMs per layer)
+        tfl = flop / (kms * 1e-3) / 1e12
+        hbm_line = {"bound": "hbm", "kernel": "fused backward (tcgen05), atdf_project_backward timed alone",
+                    "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "algorithmic_bytes": nbytes, "kernel_ms": kms,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                    else "fallback 6650 GB/s"}
+        tensor_line = {"bound": "tensor", "kernel": "fused backward (tcgen05 decoder GEMMs)", "achieved": tfl,
+                       "peak": tpeak, "unit": "TFLOP/s", "frac": tfl / tpeak, "flop_per_launch": flop,
+                       "flop_per_sample": 3 * flop_fwd,
+                       "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
+                       if "bf16_tflops_sustained" in peaks else "fallback 1400 TFLOP/s (sustained)"}
+        return hbm_line, tensor_line
+
+    roof5, troof5 = rooflines(cfg, n_slots, nseg, nsamp, r5)
+    roof2, troof2 = rooflines(cfg2, n_slots2, nseg2, nsamp2, r2)
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
+    # tcgen05 backward launch on the depth-4 workload at 16384 rays, from a
+    # single-pass ncu capture (its summary is named in traffic_source); the
+    # gradient writes still in L2 when the kernel ends are not counted there
+    roof2["traffic"] = 129719040 + 179244288 if R == 16384 else None
+    roof2["traffic_source"] = "profiles/tc_backward_dram_c2_16384rays.md" if R == 16384 else None
+    roof5["traffic"] = None
     # this library's kernels per uniform training step of the BF16 form: 13 for
     # sampling, bucketing (with the slot order), projection and loss, and one
     # Adam launch for the 12 parameters
     launches_per_step = 15
-    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
-    # tcgen05 backward launch on this workload at 16384 rays, from a
-    # single-pass ncu capture of the bench's warm-up step; the gradient
-    # writes still in L2 when the kernel ends are not counted there
-    traffic = 129719040 + 179244288 if (R == 16384 and dom_name == "backward") else None
+    h2d = sum(t.numel() * t.element_size() for t in make_host_shapes(R))
     line = {
         "metric": METRIC,
         "value": world * R / (ms * 1e-3),
@@ -492,36 +696,53 @@ def run_ours(args, rank, world):
         "vs_baseline": None,
         "dtype": "bf16",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD.replace(", FP32", ""), "rays_per_gpu_step": R,
-                   "samples_per_step": int(sg.num_samples), "segments_per_step": int(sg.num_segments),
-                   "leaves": n_slots, "parallelism": f"ray data parallel x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (114 MB BF16 factors read and 227 MB of FP32 gradients written "
-                         "per step, 908 MB of FP32 Adam state)",
-                   "form": "chosen: BF16 factors, tcgen05 decoder GEMMs (FP32 accumulation), hand-written "
-                           "adjoint, fused leaf-major; Adam on FP32 masters"},
+        "config": shared_config(cfg, n_slots, nseg, nsamp),
+        "parallelism": f"ray data parallel x{world}" if world > 1 else "single GPU",
+        "form": "chosen: BF16 factors, tcgen05 decoder GEMMs (FP32 accumulation), hand-written adjoint, fused "
+                "leaf-major; Adam on FP32 masters",
         "e2e": {"value": world * R / (ms_e2e * 1e-3), "unit": "rays/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 8},
-        "roofline": {"bound": "hbm", "kernel": f"fused {dom_name} (tcgen05)", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "algorithmic_bytes": dom_bytes,
-                     "kernel_ms": dom_ms,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650",
-                     "copy_gbs_this_gpu": copy_gbs},
-        "kernels_ms": {"fused_forward_call": tf, "fused_backward_call": tb},
-        "plain_fp32": {"value": world * R / (ms32 * 1e-3), "unit": "rays/s", "ms_per_step": ms32,
-                       "e2e_value": world * R / (ms32_e2e * 1e-3),
-                       "kernels_ms": {"fused_forward_call": tf32, "fused_backward_call": tb32}},
-        "speedup_vs_plain_fp32": ms32 / ms,
+        "roofline": {**roof5, "copy_gbs_this_gpu": copy_gbs},
+        "roofline_tensor": troof5,
+        "kernels_ms": {k: r5[k] for k in ("forward_call_ms", "backward_call_ms", "forward_entry_ms",
+                                          "backward_entry_ms")},
+        "samples_per_s": world * nsamp / (ms * 1e-3),
         "gpu_launches": launches_per_step * args.steps,
-        "clocks": clocks,
-        "samples_per_s": world * sg.num_samples / (ms * 1e-3),
+        "clocks": r5["clocks"],
+        "c2": {"workload": workload_name(cfg2), "leaves": n_slots2, "samples_per_step": nsamp2,
+               "segments_per_step": nseg2,
+               "bf16": {"value": world * R / (ms2 * 1e-3), "ms_per_step": ms2,
+                        "e2e_value": world * R / (r2["ms_e2e"] * 1e-3),
+                        "kernels_ms": {k: r2[k] for k in ("forward_call_ms", "backward_call_ms",
+                                                          "forward_entry_ms", "backward_entry_ms")},
+                        "roofline": roof2, "roofline_tensor": troof2},
+               "plain_fp32": {"value": world * R / (ms2_32 * 1e-3), "ms_per_step": ms2_32,
+                              "e2e_value": world * R / (r2_32["ms_e2e"] * 1e-3),
+                              "kernels_ms": {k: r2_32[k] for k in ("forward_call_ms", "backward_call_ms",
+                                                                   "forward_entry_ms", "backward_entry_ms")}},
+               "speedup_bf16_vs_plain_fp32": ms2_32 / ms2},
     }
-    if prop:
-        line["proposal_form"] = prop
+    if prop5:
+        line["proposal_form"] = prop5
+    if prop2:
+        line["c2"]["proposal_form"] = {**prop2, "note": "the proposal is used only while its projection error "
+                                       "against the uniform judge is <= 1%"}
     if psnr:
         line["seconds_to_psnr"] = psnr
+    if psnr30:
+        line["seconds_to_30db"] = psnr30
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_rays, 3)
+        t = oracle_tree(cfg)
+        line["cpu_baseline"] = cpu_baseline(cfg, t, args.cpu_rays, 3)
     print(json.dumps(line), flush=True)
+
+
+def make_host_shapes(R):
+    """The host tensors one e2e step copies: origin and direction [R, 3] and
+    the target [1, R], float32."""
+    import torch
+
+    return [torch.empty(R, 3), torch.empty(R, 3), torch.empty(1, R)]
 
 
 def main():

@@ -443,6 +443,18 @@ def accumulate_loss_per_node(samples, per_ray_loss, num_nodes):
     return ls, ws
 
 
+def gradient_correction_bwd(direction, ray_index, grad, dtype=np.float32):
+    """Backward of GradientCorrection
+    (hyperacorn/csrc/modules/GradientCorrection.cu:22-48): per sample i with
+    ray r = ray_index[i], g - (g . d) d with d = direction[r] as given (the
+    reference does not normalise it). The dot product is summed left to
+    right, every operation rounded to dtype on its own."""
+    d = np.asarray(direction, dtype)[np.asarray(ray_index, np.int64)]
+    g = np.asarray(grad, dtype)
+    dot = (g[:, 0] * d[:, 0] + g[:, 1] * d[:, 1]) + g[:, 2] * d[:, 2]
+    return g - dot[:, None] * d
+
+
 def num_threads():
     return lib().orc_num_threads()
 

@@ -248,3 +248,43 @@ def test_mse_loss_and_grad():
     loss, g = ab.MseLossAndGrad(x, y, 1.0)
     assert abs(loss.item() - ((x - y) ** 2).mean().item()) < 1e-6
     assert torch.allclose(g, 2 * (x - y) / 1000, atol=1e-7)
+
+
+def test_gradient_correction_bit_exact(oracle):
+    """GradientCorrection (identity forward, g - (g.d) d backward) through the
+    autograd op and through the C ABI, bit-exact against the oracle; an
+    out-of-range ray index sets the index bit and leaves its row unwritten."""
+    import ctypes as ct
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import capi
+
+    rng = np.random.default_rng(5)
+    R, S = 300, 20000
+    d = rng.normal(size=(R, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    ray = rng.integers(0, R, S)
+    pos = rng.uniform(-1, 1, (S, 3)).astype(np.float32)
+    g = rng.normal(size=(S, 3)).astype(np.float32)
+    pt = torch.from_numpy(pos).cuda().requires_grad_(True)
+    out = ab.GradientCorrection(pt, torch.from_numpy(d).cuda(), torch.from_numpy(ray).cuda())
+    assert torch.equal(out.detach(), pt.detach())
+    out.backward(torch.from_numpy(g).cuda())
+    ref = oracle.gradient_correction_bwd(d, ray, g)
+    assert np.array_equal(pt.grad.cpu().numpy(), ref)
+
+    L = capi.lib()
+    ray_bad = ray.copy()
+    ray_bad[7] = R + 3
+    dt, rt, gt = (torch.from_numpy(x).cuda() for x in (d, ray_bad, g))
+    gout = torch.full((S, 3), 123.0, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.atdf_gradient_correction_backward(capi.ptr(dt), capi.ptr(rt), R, capi.ptr(gt), S, capi.ptr(gout),
+                                               capi.ptr(err), stream) == 0
+    torch.cuda.synchronize()
+    assert err.item() == capi.DEVERR["index"]
+    got = gout.cpu().numpy()
+    assert np.all(got[7] == 123.0)
+    keep = np.arange(S) != 7
+    assert np.array_equal(got[keep], ref[keep])

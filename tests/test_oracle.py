@@ -229,3 +229,28 @@ def test_jitter_hash_and_node_error(oracle):
     expect = np.zeros_like(ls)
     np.add.at(expect, s["node_id"], prl[0][s["ray_index"]].astype(np.float64) * s["weight"])
     assert np.allclose(ls, expect)
+
+
+def test_gradient_correction_known_answers(oracle):
+    """GradientCorrection's backward removes the gradient's component along
+    the ray (GradientCorrection.cu:22-48): for a unit direction the result is
+    orthogonal to it, a second application changes nothing, and a gradient
+    along the ray vanishes. Axis-aligned cases are exact in FP32."""
+    rng = np.random.default_rng(3)
+    R, S = 50, 2000
+    d = rng.normal(size=(R, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    ray = rng.integers(0, R, S)
+    g = rng.normal(size=(S, 3))
+    out = oracle.gradient_correction_bwd(d, ray, g, np.float64)
+    assert np.abs((out * d[ray]).sum(1)).max() < 1e-12
+    again = oracle.gradient_correction_bwd(d, ray, out, np.float64)
+    assert np.abs(again - out).max() < 1e-12
+    along = oracle.gradient_correction_bwd(d, ray, 2.5 * d[ray], np.float64)
+    assert np.abs(along).max() < 1e-12
+    # FP32 restatement within rounding of the FP64 one
+    out32 = oracle.gradient_correction_bwd(d.astype(np.float32), ray, g.astype(np.float32), np.float32)
+    assert out32.dtype == np.float32 and np.abs(out32 - out).max() < 1e-5
+    ax = np.array([[0.0, 0.0, 1.0]], np.float32)
+    gg = np.array([[1.5, -2.0, 7.0]], np.float32)
+    assert np.array_equal(oracle.gradient_correction_bwd(ax, [0], gg), np.array([[1.5, -2.0, 0.0]], np.float32))
