@@ -67,8 +67,9 @@ class HyperTreeBase {
     std::tuple<torch::Tensor, torch::Tensor> NodeIdForPositionGPU(torch::Tensor global_samples);
     void SetErrorForActiveNodes(torch::Tensor error, const std::string& strategy);
     // Tree structure optimisation (HyperTreeStructureOptimizer.cpp:5-392,
-    // OR-Tools MIP in the reference) solved greedily on the host: split / merge
-    // active leaves under a budget of active leaves, costs from node_error and
+    // an OR-Tools MIP in the reference) solved exactly on the host by dynamic
+    // programming over the active-leaf count: split / merge / keep active
+    // leaves under a budget of active leaves, costs from node_error and
     // node_max_density. Returns whether the structure changed (then the active
     // set, prefix sums and flags are updated).
     bool OptimizeStructure(int64_t max_active_nodes, double error_merge_factor = 1.1,

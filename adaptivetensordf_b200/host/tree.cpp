@@ -4,7 +4,9 @@
 #include <ATen/cuda/CUDAContext.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "atdf_host.h"
@@ -391,18 +393,55 @@ void HyperTreeBase::SetErrorForActiveNodes(torch::Tensor error, const std::strin
 }
 
 // ---------------------------------------------------------------------------
-// Tree structure optimisation. The reference solves a mixed-integer program
-// with OR-Tools / CBC (HyperTreeStructureOptimizer.cpp:5-392): every active
-// leaf chooses none / split / merge (all active siblings together), the cost
-// of a choice is error x max density with the split and merge predictions of
-// :211-323 (split: error_split_factor x own error; merge: error_merge_factor x
-// the siblings' error sum, at the siblings' max density), and the active-leaf
-// count after the change must stay within max_active_nodes (:146-206). OR-Tools
-// is not available, so the same program is solved greedily: merges with the
-// smallest cost increase per freed leaf until the budget holds, then splits
-// by gain per added leaf, paying for a split with cheaper merges while that
-// lowers the objective.
+// Structure optimisation. The reference solves a mixed-integer program with
+// OR-Tools / CBC (HyperTreeStructureOptimizer.cpp:5-392): every active leaf
+// chooses none / split / merge, where a merge takes all siblings of a group
+// whose members are all active or culled (:146-182), a split needs children
+// (:102-106, :185-196), the cost of a choice is error x max density with the
+// split and merge predictions of :211-323 (none: own error at own density;
+// split: error_split_factor x own error at own density; merge:
+// error_merge_factor x the siblings' error sum at their max density), and the
+// active-leaf count after the change (none 1, split its non-culled children,
+// merge 1 per group) must stay within max_active_nodes (:136-206).
+//
+// The program is a multiple-choice knapsack over independent items: each
+// mergeable sibling group (merge, or each member none / split) and each other
+// active leaf (none / split). It is solved exactly by dynamic programming
+// over the leaf count: per group a table of the cheapest member choices for
+// every count, plus the merge at count 1; then the groups and leaves are
+// combined count by count, keeping each item's choice for the backtrack.
+// When no choice meets the budget the smallest possible leaf count is taken.
 // ---------------------------------------------------------------------------
+namespace {
+
+// Cost of a set of choices and how many leaves or groups they change: among
+// choices whose costs agree to 1e-12 the one with fewer changes is preferred
+// (no change without a gain).
+struct Score {
+    double cost;
+    int changes;
+};
+
+bool better(const Score& a, const Score& b)
+{
+    const double inf = std::numeric_limits<double>::infinity();
+    if (b.cost == inf) return a.cost < inf;
+    if (a.cost == inf) return false;
+    const double tol = 1e-12 * std::max(std::fabs(a.cost), std::fabs(b.cost));
+    if (a.cost < b.cost - tol) return true;
+    if (b.cost < a.cost - tol) return false;
+    return a.changes < b.changes;
+}
+
+// Leaf choices: none (count 1) and, when it has live children, split.
+struct LeafItem {
+    int64_t node;
+    double none, split;
+    int live;  // non-culled children (0: cannot split)
+};
+
+}  // namespace
+
 bool HyperTreeBase::OptimizeStructure(int64_t max_active_nodes, double error_merge_factor,
                                       double error_split_factor)
 {
@@ -410,7 +449,6 @@ bool HyperTreeBase::OptimizeStructure(int64_t max_active_nodes, double error_mer
     auto act_t = node_active.to(torch::kCPU).contiguous().clone();
     auto cul_t = node_culled.to(torch::kCPU).contiguous();
     auto chd_t = node_children.to(torch::kCPU).contiguous();
-    auto par_t = node_parent.to(torch::kCPU).contiguous();
     auto err_t = node_error.to(torch::kCPU).to(torch::kFloat64).contiguous();
     auto den_t = node_max_density.to(torch::kCPU).to(torch::kFloat64).contiguous();
     const int64_t n = act_t.size(0);
@@ -418,127 +456,167 @@ bool HyperTreeBase::OptimizeStructure(int64_t max_active_nodes, double error_mer
     int32_t* act = act_t.data_ptr<int32_t>();
     const int32_t* cul = cul_t.data_ptr<int32_t>();
     const int32_t* chd = chd_t.data_ptr<int32_t>();
-    const int32_t* par = par_t.data_ptr<int32_t>();
     const double* err = err_t.data_ptr<double>();
     const double* den = den_t.data_ptr<double>();
     auto e_of = [&](int64_t i) { return err[i] > 0 ? err[i] : 0.0; };
     // a density never computed (negative) counts as 1
     auto d_of = [&](int64_t i) { return den[i] >= 0 ? den[i] : 1.0; };
-
-    struct Split {
-        int64_t node;
-        double gain;
-        int cost;  // leaves added
-    };
-    struct Merge {
-        int64_t parent;
-        double loss;
-        int freed;  // leaves removed
-    };
-    std::vector<Split> splits;
-    std::vector<Merge> merges;
-    int64_t count = 0;
-    for (int64_t i = 0; i < n; ++i) {
-        if (act[i] != 1) continue;
-        ++count;
+    auto leaf_item = [&](int64_t i) {
+        LeafItem it{i, e_of(i) * d_of(i), 0.0, 0};
         if (chd[i * ns] >= 0) {
-            int live = 0;
-            for (int k = 0; k < ns; ++k) live += cul[chd[i * ns + k]] ? 0 : 1;
-            if (live > 0) {
-                const double none = e_of(i) * d_of(i);
-                const double split = error_split_factor * e_of(i) * d_of(i);
-                splits.push_back({i, none - split, live - 1});
-            }
+            for (int k = 0; k < ns; ++k) it.live += cul[chd[i * ns + k]] ? 0 : 1;
+            it.split = error_split_factor * e_of(i) * d_of(i);
         }
-    }
+        return it;
+    };
+
+    // items: mergeable groups (members + merge cost) and single leaves
+    struct Group {
+        int64_t parent;  // -1: a single leaf
+        std::vector<LeafItem> members;
+        double merge;
+    };
+    std::vector<Group> items;
+    std::vector<char> in_group(n, 0);
     for (int64_t p = 0; p < n; ++p) {
-        if (chd[p * ns] < 0) continue;
+        if (chd[p * ns] < 0 || act[p] == 1) continue;
         int active = 0, culled = 0;
-        double esum = 0, dmax = 0, none = 0;
         for (int k = 0; k < ns; ++k) {
             const int32_t c = chd[p * ns + k];
-            if (act[c] == 1) {
-                ++active;
-                esum += e_of(c);
-                dmax = std::max(dmax, d_of(c));
-                none += e_of(c) * d_of(c);
-            } else if (cul[c]) {
-                ++culled;
-            }
+            active += act[c] == 1;
+            culled += (act[c] != 1 && cul[c]) ? 1 : 0;
         }
         if (active == 0 || active + culled != ns) continue;
-        merges.push_back({p, error_merge_factor * esum * dmax - none, active - 1});
+        Group g{p, {}, 0.0};
+        double esum = 0, dmax = 0;
+        for (int k = 0; k < ns; ++k) {
+            const int32_t c = chd[p * ns + k];
+            if (act[c] != 1) continue;
+            g.members.push_back(leaf_item(c));
+            esum += e_of(c);
+            dmax = std::max(dmax, d_of(c));
+            in_group[c] = 1;
+        }
+        g.merge = error_merge_factor * esum * dmax;
+        items.push_back(std::move(g));
     }
-    std::sort(splits.begin(), splits.end(), [](const Split& a, const Split& b) {
-        return a.gain * std::max(b.cost, 1) > b.gain * std::max(a.cost, 1);
-    });
-    std::sort(merges.begin(), merges.end(), [](const Merge& a, const Merge& b) {
-        return a.loss * std::max(b.freed, 1) < b.loss * std::max(a.freed, 1);
-    });
-    std::vector<char> split_taken(n, 0), merge_taken(n, 0), blocked(n, 0);  // blocked: parent of a split leaf
-    size_t mi = 0;
-    auto next_merge = [&]() -> int64_t {
-        while (mi < merges.size() && (blocked[merges[mi].parent] || merge_taken[merges[mi].parent])) ++mi;
-        return mi < merges.size() ? (int64_t)mi : -1;
+    for (int64_t i = 0; i < n; ++i) {
+        if (act[i] != 1) continue;
+        if (!in_group[i]) items.push_back(Group{-1, {leaf_item(i)}, 0.0});
+    }
+
+    // per item: the cheapest member choices for every leaf count (member
+    // sub-table with its own backtrack), plus the merge at count 1
+    const Score none_yet{std::numeric_limits<double>::infinity(), 0};
+    auto reachable = [](const Score& x) { return x.cost < std::numeric_limits<double>::infinity(); };
+    struct Table {
+        int hi;                               // counts 1..hi
+        std::vector<Score> score;             // [hi + 1]
+        std::vector<char> merged;             // the count-1 entry is the merge
+        std::vector<std::vector<char>> pick;  // [member][count]: member splits
     };
-    // 1. meet the budget
-    while (count > max_active_nodes) {
-        const int64_t k = next_merge();
-        if (k < 0) break;
-        merge_taken[merges[k].parent] = 1;
-        count -= merges[k].freed;
-        ++mi;
+    std::vector<Table> tables(items.size());
+    int64_t lo_total = 0, hi_total = 0;
+    for (size_t gi = 0; gi < items.size(); ++gi) {
+        const Group& g = items[gi];
+        Table& t = tables[gi];
+        int hi = 0;
+        for (const LeafItem& m : g.members) hi += std::max(1, m.live);
+        std::vector<Score> cur(hi + 1, none_yet), nxt(hi + 1, none_yet);
+        cur[0] = Score{0.0, 0};
+        t.pick.assign(g.members.size(), std::vector<char>(hi + 1, 0));
+        int reach = 0;
+        for (size_t mi = 0; mi < g.members.size(); ++mi) {
+            const LeafItem& m = g.members[mi];
+            std::fill(nxt.begin(), nxt.end(), none_yet);
+            for (int b = 0; b <= reach; ++b) {
+                if (!reachable(cur[b])) continue;
+                const Score keep{cur[b].cost + m.none, cur[b].changes};
+                if (better(keep, nxt[b + 1])) {
+                    nxt[b + 1] = keep;
+                    t.pick[mi][b + 1] = 0;
+                }
+                const Score split{cur[b].cost + m.split, cur[b].changes + 1};
+                if (m.live > 0 && better(split, nxt[b + m.live])) {
+                    nxt[b + m.live] = split;
+                    t.pick[mi][b + m.live] = 1;
+                }
+            }
+            reach += std::max(1, m.live);
+            std::swap(cur, nxt);
+        }
+        t.hi = hi;
+        t.score = cur;
+        t.merged.assign(hi + 1, 0);
+        if (g.parent >= 0 && better(Score{g.merge, 1}, t.score[1])) {
+            t.score[1] = Score{g.merge, 1};
+            t.merged[1] = 1;
+        }
+        int lo = hi;
+        for (int b = 1; b <= hi; ++b)
+            if (reachable(t.score[b])) lo = std::min(lo, b);
+        lo_total += lo;
+        hi_total += hi;
     }
-    // 2. splits, paid for by merges when the budget is full
-    for (const Split& sp : splits) {
-        if (sp.gain <= 0) break;
-        const int64_t parent = par[sp.node];
-        if (parent >= 0 && merge_taken[parent]) continue;  // its sibling group is being merged
-        if (count + sp.cost <= max_active_nodes) {
-            split_taken[sp.node] = 1;
-            if (parent >= 0) blocked[parent] = 1;
-            count += sp.cost;
+    const int64_t B = std::max<int64_t>(std::min<int64_t>(max_active_nodes, hi_total), lo_total);
+
+    // combine the items count by count: best[b] = cheapest choices at count b
+    std::vector<Score> best(B + 1, none_yet), next(B + 1, none_yet);
+    best[0] = Score{0.0, 0};
+    std::vector<std::vector<int32_t>> choice(items.size());  // count taken by item gi at total b
+    int64_t reach = 0;
+    for (size_t gi = 0; gi < items.size(); ++gi) {
+        const Table& t = tables[gi];
+        std::fill(next.begin(), next.end(), none_yet);
+        choice[gi].assign(B + 1, -1);
+        for (int64_t b = 0; b <= std::min(reach, B); ++b) {
+            if (!reachable(best[b])) continue;
+            for (int c = 1; c <= t.hi && b + c <= B; ++c) {
+                if (!reachable(t.score[c])) continue;
+                const Score v{best[b].cost + t.score[c].cost, best[b].changes + t.score[c].changes};
+                if (better(v, next[b + c])) {
+                    next[b + c] = v;
+                    choice[gi][b + c] = c;
+                }
+            }
+        }
+        reach += t.hi;
+        std::swap(best, next);
+    }
+    int64_t bstar = -1;
+    for (int64_t b = 0; b <= B; ++b)
+        if (reachable(best[b]) && (bstar < 0 || better(best[b], best[bstar]))) bstar = b;
+    TORCH_CHECK(bstar >= 0, "OptimizeStructure: no feasible leaf count");
+
+    // backtrack and apply
+    bool changed = false;
+    int64_t b = bstar;
+    for (size_t gi = items.size(); gi-- > 0;) {
+        const Group& g = items[gi];
+        const Table& t = tables[gi];
+        const int c = choice[gi][b];
+        TORCH_CHECK(c >= 1, "OptimizeStructure: backtrack failed");
+        b -= c;
+        if (t.merged[c]) {
+            for (const LeafItem& m : g.members) act[m.node] = 0;
+            act[g.parent] = 1;
+            changed = true;
             continue;
         }
-        // merges needed to make room, cheapest first, none involving this leaf
-        const char was_blocked = parent >= 0 ? blocked[parent] : 0;
-        if (parent >= 0) blocked[parent] = 1;
-        std::vector<int64_t> pick;
-        double loss = 0;
-        int64_t freed = 0;
-        size_t save = mi;
-        while (count + sp.cost - freed > max_active_nodes) {
-            const int64_t k = next_merge();
-            if (k < 0) break;
-            pick.push_back(k);
-            loss += merges[k].loss;
-            freed += merges[k].freed;
-            ++mi;
-        }
-        if (count + sp.cost - freed <= max_active_nodes && loss < sp.gain) {
-            for (int64_t k : pick) merge_taken[merges[k].parent] = 1;
-            split_taken[sp.node] = 1;
-            count += sp.cost - freed;
-        } else {
-            mi = save;
-            if (parent >= 0) blocked[parent] = was_blocked;
-            break;
-        }
-    }
-    bool changed = false;
-    for (int64_t i = 0; i < n; ++i) {
-        if (split_taken[i]) {
-            act[i] = 0;
-            for (int k = 0; k < ns; ++k) {
-                const int32_t c = chd[i * ns + k];
-                if (!cul[c]) act[c] = 1;
+        int r = c;
+        for (size_t mi = g.members.size(); mi-- > 0;) {
+            const LeafItem& m = g.members[mi];
+            if (t.pick[mi][r]) {
+                act[m.node] = 0;
+                for (int k = 0; k < ns; ++k) {
+                    const int32_t ch = chd[m.node * ns + k];
+                    if (!cul[ch]) act[ch] = 1;
+                }
+                r -= m.live;
+                changed = true;
+            } else {
+                r -= 1;
             }
-            changed = true;
-        }
-        if (merge_taken[i]) {
-            for (int k = 0; k < ns; ++k) act[chd[i * ns + k]] = 0;
-            act[i] = 1;
-            changed = true;
         }
     }
     if (changed) {
