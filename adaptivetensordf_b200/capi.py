@@ -195,6 +195,8 @@ def _declare(L):
         "atdf_adam_step": (I32, [I64, P, P, P, P, P, F32, F32, F32, F32, F32, I64, P]),
         "atdf_adam_step_multi": (I32, [I32, P, P]),
         "atdf_camera_rays": (I32, [I64, P, P, P, P, P, I64, P, I64, I32, I32, I32, I32, P, P, P, P, P]),
+        "atdf_point_in_any_image": (I32, [I64, P, P, P, I64, P, I32, I32, I32, ct.POINTER(F32),
+                                          ct.POINTER(F32), P, P]),
         "atdf_tone_map_forward": (I32, [ct.POINTER(ToneMapper), I64, I64, P, P, P, P, P, P]),
         "atdf_tone_map_backward": (I32, [ct.POINTER(ToneMapper), I64, I64, P, P, P, P, P, P, P, P, P, P]),
         "atdf_tone_response_loss": (I32, [I32, P, F32, P, P, P, P]),

@@ -85,9 +85,69 @@ __global__ void camera_rays_kernel(int64_t n, const float* __restrict__ uv, cons
     }
 }
 
+// SceneBase::PointInAnyImage (hyperacorn/csrc/data/SceneBase.cu:13-97): a
+// point is marked when it lies in the ROI box (closed bounds on its FP32
+// value, BoxContainsPoint, HyperTree.h:382-392) and its projection rounds to a
+// pixel inside the w x h image of at least one pose. The view position is
+// R^T (p - t) in FP64 (the pose's unit quaternion R conjugated, t its
+// translation or zero), the pixel is (fx v.x + cx, fy v.y + cy) for the
+// orthographic camera and (fx v.x / v.z + cx, fy v.y / v.z + cy) for the
+// pinhole one (the skew set to zero as the reference does), rounded half away
+// from zero. One thread per point, images in order until one contains it.
+__global__ void point_in_any_image_kernel(int64_t n, const float* __restrict__ pts,
+                                          const double* __restrict__ rotation, const double* __restrict__ translation,
+                                          int64_t num_images, const double* __restrict__ K, int model, int w, int h,
+                                          float3 rmin, float3 rmax, float* __restrict__ mask)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = pts[3 * i], y = pts[3 * i + 1], z = pts[3 * i + 2];
+        float m = 0.0f;
+        if (!(rmin.x > x || rmax.x < x || rmin.y > y || rmax.y < y || rmin.z > z || rmax.z < z)) {
+            for (int64_t a = 0; a < num_images && m == 0.0f; ++a) {
+                const double* q = rotation + 4 * a;
+                const double qi[4] = {-q[0], -q[1], -q[2], q[3]};
+                D3 pt{(double)x, (double)y, (double)z};
+                if (translation) {
+                    const double* t = translation + 3 * a;
+                    pt = {__dsub_rn(pt.x, t[0]), __dsub_rn(pt.y, t[1]), __dsub_rn(pt.z, t[2])};
+                }
+                const D3 v = rotate(qi, pt);
+                double px, py;
+                if (model == ATDF_CAMERA_ORTHOGRAPHIC) {
+                    px = __dadd_rn(__dmul_rn(K[0], v.x), K[2]);
+                    py = __dadd_rn(__dmul_rn(K[1], v.y), K[3]);
+                } else {
+                    px = __dadd_rn(__dmul_rn(K[0], __ddiv_rn(v.x, v.z)), K[2]);
+                    py = __dadd_rn(__dmul_rn(K[1], __ddiv_rn(v.y, v.z)), K[3]);
+                }
+                const double rx = round(px), ry = round(py);
+                if (rx >= 0.0 && rx < (double)w && ry >= 0.0 && ry < (double)h) m = 1.0f;
+            }
+        }
+        mask[i] = m;
+    }
+}
+
 }  // namespace atdf
 
 using namespace atdf;
+
+extern "C" int atdf_point_in_any_image(int64_t n, const float* points, const double* rotation,
+                                       const double* translation, int64_t num_images, const double* intrinsics,
+                                       int32_t width, int32_t height, int32_t model, const float* roi_min,
+                                       const float* roi_max, float* mask, atdf_stream_t stream)
+{
+    if (n < 0 || width < 1 || height < 1 || num_images < 1 || !roi_min || !roi_max) return ATDF_ERR_INVALID_ARGUMENT;
+    if (model != ATDF_CAMERA_PINHOLE && model != ATDF_CAMERA_ORTHOGRAPHIC) return ATDF_ERR_INVALID_ARGUMENT;
+    if (n > 0 && (!points || !rotation || !intrinsics || !mask)) return ATDF_ERR_INVALID_ARGUMENT;
+    if (n == 0) return ATDF_OK;
+    const unsigned blocks = (unsigned)std::min<int64_t>(div_up(n, 256), 148 * 16);
+    point_in_any_image_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(
+        n, points, rotation, translation, num_images, intrinsics, model, width, height,
+        make_float3(roi_min[0], roi_min[1], roi_min[2]), make_float3(roi_max[0], roi_max[1], roi_max[2]), mask);
+    ATDF_LAUNCH_CHECK();
+    return ATDF_OK;
+}
 
 extern "C" int atdf_camera_rays(int64_t n, const float* uv, const int32_t* image_id, const int32_t* camera_id,
                                 const double* rotation, const double* translation, int64_t num_images,

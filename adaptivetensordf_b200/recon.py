@@ -77,10 +77,39 @@ class TiltSeries:
     uv: torch.Tensor = None        # [A * P, 2] float32: the ray's pixel centre in [0, 1] (u along the width)
     height: int = 0                # detector size in pixels
     width: int = 0
+    # the cameras, for the visibility mask of the max-density grid:
+    # rotation [A, 4] unit quaternions (x, y, z, w) and translation [A, 3]
+    # (or None) float64, intrinsics fx fy cx cy s, model (0 pinhole, 1
+    # orthographic) and the ROI box
+    cam_rotation: np.ndarray = None
+    cam_translation: np.ndarray = None
+    cam_intrinsics: tuple = None
+    cam_model: int = 1
+    roi_min: tuple = (-1.0, -1.0, -1.0)
+    roi_max: tuple = (1.0, 1.0, 1.0)
 
     @property
     def num_rays(self):
         return self.origin.shape[0]
+
+
+def tilt_quaternions(angles_deg, off_axis_deg: float = 0.0):
+    """Unit quaternions (x, y, z, w) of the parallel-beam tilts: a rotation by
+    the tilt angle about y, after the specimen's off-axis rotation about x
+    (synthetic.parallel_beam_rays: d = R (0, 0, 1), origin = R (u, v, 0) -
+    sqrt(2) d)."""
+    out = []
+    ax = math.radians(off_axis_deg) / 2
+    qx = np.array([math.sin(ax), 0.0, 0.0, math.cos(ax)])
+    for a in np.asarray(angles_deg, np.float64):
+        h = math.radians(a) / 2
+        qy = np.array([0.0, math.sin(h), 0.0, math.cos(h)])
+        # q = qx * qy (Hamilton product, x y z w)
+        x1, y1, z1, w1 = qx
+        x2, y2, z2, w2 = qy
+        out.append([w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2, w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2,
+                    w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2, w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2])
+    return np.asarray(out)
 
 
 def make_tilt_series(cfg, device="cuda", noise_seed: int = 1002) -> TiltSeries:
@@ -110,8 +139,40 @@ def make_tilt_series(cfg, device="cuda", noise_seed: int = 1002) -> TiltSeries:
             y = y + torch.from_numpy(rng.normal(0.0, sigma, A * P)).to(device)
     n = cfg.detector
     uv = np.stack([(pix % n + 0.5) / n, (pix // n + 0.5) / n], 1).astype(np.float32)
+    # the parallel beam as orthographic cameras: pixel centre i maps to
+    # (i - (n - 1) / 2) / (n / 2), the detector coordinate of the rays
     return TiltSeries(o_t, d_t, y.float(), clean, vol_t, angles, torch.from_numpy(img).to(device),
-                      torch.from_numpy(uv).to(device), n, n)
+                      torch.from_numpy(uv).to(device), n, n, cam_rotation=tilt_quaternions(angles),
+                      cam_intrinsics=(n / 2, n / 2, (n - 1) / 2, (n - 1) / 2, 0.0), cam_model=1)
+
+
+def point_in_any_image(points: torch.Tensor, data: TiltSeries) -> torch.Tensor:
+    """SceneBase::PointInAnyImage (SceneBase.cu:13-97) of points [P, 3] on the
+    series' cameras: 1 where a point lies in the ROI and projects into some
+    image, else 0 (float32, on the points' device). Without cameras every
+    point counts as seen."""
+    import ctypes as ct
+
+    from . import capi
+
+    pts = points.contiguous().float()
+    if data.cam_rotation is None:
+        return torch.ones(pts.shape[0], device=pts.device)
+    dev = pts.device
+    rot = torch.from_numpy(np.ascontiguousarray(data.cam_rotation, np.float64)).to(dev)
+    tr = None if data.cam_translation is None else \
+        torch.from_numpy(np.ascontiguousarray(data.cam_translation, np.float64)).to(dev)
+    K = torch.tensor(data.cam_intrinsics, dtype=torch.float64, device=dev)
+    mask = torch.empty(pts.shape[0], device=dev)
+    lo = (ct.c_float * 3)(*data.roi_min)
+    hi = (ct.c_float * 3)(*data.roi_max)
+    st = capi.lib().atdf_point_in_any_image(pts.shape[0], capi.ptr(pts), capi.ptr(rot), capi.ptr(tr),
+                                            rot.shape[0], capi.ptr(K), data.width, data.height, data.cam_model,
+                                            lo, hi, capi.ptr(mask),
+                                            ct.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if st != 0:
+        raise RuntimeError(f"atdf_point_in_any_image: {capi.lib().atdf_status_string(st).decode()}")
+    return mask
 
 
 # ----------------------------------------------------------------------------
@@ -152,26 +213,36 @@ def psnr(tree, geo, phantom: torch.Tensor):
 _PLANE_AXES = ((1, 2, 0), (0, 2, 1), (0, 1, 2))  # plane m: (u axis, v axis, third axis)
 
 
-@torch.no_grad()
-def compute_max_density(tree, geo, g: int = 12):
-    """Per active leaf, the maximum decoded density over a g^3 grid of cell
-    centres inside it (hyper_train.cpp:662-707 ComputeMaxDensity with
-    UniformGlobalSamples); written into tree.node_max_density."""
-    ids = tree.active_node_ids
-    dev = ids.device
-    c = (torch.arange(g, device=dev, dtype=torch.float32) + 0.5) / g
-    zz, yy, xx = torch.meshgrid(c, c, c, indexing="ij")
+def uniform_global_samples(tree, node_ids: torch.Tensor, g: int = 20) -> torch.Tensor:
+    """HyperTreeBase::UniformGlobalSamples (HyperTree.cu:1618-1653): per node
+    a g^3 grid spanning its box corner to corner, local = index / (g - 1) and
+    position = local * size + min in FP32; [N, g^3, 3] with x fastest."""
+    dev = node_ids.device
+    local = torch.arange(g, device=dev, dtype=torch.float32) / float(g - 1)
+    zz, yy, xx = torch.meshgrid(local, local, local, indexing="ij")
     unit = torch.stack([xx, yy, zz], -1).reshape(-1, 3)
-    mx = torch.empty(ids.numel(), device=dev)
-    chunk = max(1, (1 << 21) // unit.shape[0])
+    mn = tree.node_position_min[node_ids]
+    sz = tree.node_position_max[node_ids] - mn
+    return unit[None] * sz[:, None, :] + mn[:, None, :]
+
+
+@torch.no_grad()
+def compute_max_density(tree, geo, data: TiltSeries = None, g: int = 20):
+    """Per active leaf, the maximum decoded density over its g^3 corner-to-
+    corner grid, each point masked by the series' visibility
+    (hyper_train.cpp:662-707 ComputeMaxDensity: grid 20 for the VM geometry,
+    PointInAnyImage); written into tree.node_max_density."""
+    ids = tree.active_node_ids
+    mx = torch.empty(ids.numel(), device=ids.device)
+    chunk = max(1, (1 << 21) // (g * g * g))
     for i in range(0, ids.numel(), chunk):
         nid = ids[i:i + chunk]
-        mn = tree.node_position_min[nid]
-        sz = tree.node_position_max[nid] - mn
-        pts = (mn[:, None, :] + unit[None] * sz[:, None, :]).reshape(-1, 3).contiguous()
-        node = nid[:, None].expand(-1, unit.shape[0]).reshape(-1).contiguous()
-        dens = geo.SampleVolumeIndirect(tree, pts, node).reshape(nid.numel(), -1)
-        mx[i:i + chunk] = dens.max(1).values
+        pts = uniform_global_samples(tree, nid, g).reshape(-1, 3).contiguous()
+        node = nid[:, None].expand(-1, g * g * g).reshape(-1).contiguous()
+        dens = geo.SampleVolumeIndirect(tree, pts, node).reshape(-1)
+        if data is not None:
+            dens = dens * point_in_any_image(pts, data)
+        mx[i:i + chunk] = dens.reshape(nid.numel(), -1).max(1).values
     md = tree.node_max_density.clone()
     md[ids] = mx.to(md.device)
     tree.node_max_density = md
@@ -261,7 +332,7 @@ def refine(tree, geo, data: TiltSeries, max_active_nodes: int, max_samples_per_n
     leaves. Returns whether the tree changed; the caller resets the optimizer
     (reset_optimizer_after_structure_change)."""
     node_errors(tree, geo, data, max_samples_per_node)
-    compute_max_density(tree, geo)
+    compute_max_density(tree, geo, data)
     old_tree = _tree_like(tree, tree.node_active)
     old_planes = [p.detach() for p in geo.planes]
     if not tree.OptimizeStructure(max_active_nodes, error_merge_factor, error_split_factor):

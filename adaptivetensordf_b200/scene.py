@@ -190,7 +190,13 @@ class Scene:
         if vf.endswith(".npy"):
             vol = torch.from_numpy(np.load(os.path.join(self.path, vf)).astype(np.float32)).to(device)
         angles = self.angles if self.angles is not None else np.zeros(A)
-        return TiltSeries(o, d, y, y.double(), vol, angles, iid, uv, h, w)
+        # PointInAnyImage uses the first camera's intrinsics (SceneBase.cu:19-23)
+        return TiltSeries(o, d, y, y.double(), vol, angles, iid, uv, h, w,
+                          cam_rotation=np.asarray(self.rotation, np.float64),
+                          cam_translation=np.asarray(self.translation, np.float64),
+                          cam_intrinsics=tuple(np.asarray(self.intrinsics, np.float64)[0].tolist()),
+                          cam_model=CAMERA_MODELS[self.params.camera_model],
+                          roi_min=tuple(self.params.roi_min), roi_max=tuple(self.params.roi_max))
 
 
 def load_scene(path: str) -> Scene:

@@ -444,6 +444,19 @@ int atdf_camera_rays(int64_t n, const float* uv, const int32_t* image_id, const 
                      const float* volume_translation, float* origin, float* direction, int32_t* dev_error,
                      atdf_stream_t stream);
 
+/* SceneBase::PointInAnyImage (hyperacorn/csrc/data/SceneBase.cu:13-97), the
+ * visibility mask of the per-leaf max-density grid: mask[i] = 1 when point i
+ * ([n, 3] float) lies in the ROI box [roi_min, roi_max] (host float[3] each,
+ * closed bounds) and projects to a pixel of at least one of the num_images
+ * poses (rotation [num_images, 4] unit quaternions x y z w, translation
+ * [num_images, 3] or null = 0; view = R^T (p - t), intrinsics [5] = fx fy cx
+ * cy s with the skew ignored, pixel rounded half away from zero, inside
+ * [0, width) x [0, height)); else 0. */
+int atdf_point_in_any_image(int64_t n, const float* points, const double* rotation, const double* translation,
+                            int64_t num_images, const double* intrinsics, int32_t width, int32_t height,
+                            int32_t model, const float* roi_min, const float* roi_max, float* mask,
+                            atdf_stream_t stream);
+
 /* ---- optimizer step ------------------------------------------------------
  * Replaces the torch::optim::Adam step the reference builds for the grid and
  * decoder parameters (geometry_tensor_qo.cpp:79-81, 209-220): torch's Adam

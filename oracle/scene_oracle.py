@@ -11,6 +11,7 @@ Follows the reference:
   * quaternion rotation of a point (Saiga/Eigen unit quaternion x, y, z, w)
   * SceneBase::GetRays        hyperacorn/csrc/data/SceneBase.cpp:369-450
   * SceneBase::LoadImagesCT   hyperacorn/csrc/data/SceneBase.cpp:904-975
+  * SceneBase::PointInAnyImage hyperacorn/csrc/data/SceneBase.cu:13-97
 Parity unpinned: the reference ships no test vectors for these; the
 restatement is checked against the synthetic parallel-beam geometry and
 against closed forms in the tests.
@@ -87,3 +88,38 @@ def tilt_quaternion(angle_deg):
     """Unit quaternion (x, y, z, w) of a rotation by angle about the y axis."""
     a = math.radians(angle_deg) / 2
     return np.array([0.0, math.sin(a), 0.0, math.cos(a)])
+
+
+def _round_half_away(x):
+    """C's round(): to the nearest integer, halves away from zero (the
+    fractional part x - trunc(x) is exact in FP64)."""
+    r = np.trunc(x)
+    return r + np.where(np.abs(x - r) >= 0.5, np.sign(x), 0.0)
+
+
+def point_in_any_image(points, rotation, translation, intrinsics, w, h, model, roi_min, roi_max):
+    """Visibility mask [n] float32 of SceneBase::PointInAnyImage: 1 where the
+    point lies in the closed ROI box (FP32 comparison, BoxContainsPoint,
+    HyperTree.h:382-392) and R^T (p - t) (FP64, the conjugate quaternion)
+    projects, rounded half away from zero, into [0, w) x [0, h) for some pose
+    (orthographic: fx v.x + cx, fy v.y + cy; pinhole: fx v.x / v.z + cx,
+    fy v.y / v.z + cy; the skew ignored as the reference sets it to 0)."""
+    pts = np.asarray(points, np.float32)
+    lo = np.asarray(roi_min, np.float32)
+    hi = np.asarray(roi_max, np.float32)
+    inside = np.all((lo[None] <= pts) & (pts <= hi[None]), axis=1)
+    p64 = pts.astype(np.float64)
+    K = np.asarray(intrinsics, np.float64)
+    rot = np.asarray(rotation, np.float64)
+    mask = np.zeros(len(pts), bool)
+    for a in range(len(rot)):
+        qi = np.tile(rot[a] * np.array([-1.0, -1.0, -1.0, 1.0]), (len(pts), 1))
+        p = p64 - np.asarray(translation, np.float64)[a][None] if translation is not None else p64
+        v = rotate(qi, p)
+        if model == 1:
+            px, py = K[0] * v[:, 0] + K[2], K[1] * v[:, 1] + K[3]
+        else:
+            px, py = K[0] * (v[:, 0] / v[:, 2]) + K[2], K[1] * (v[:, 1] / v[:, 2]) + K[3]
+        rx, ry = _round_half_away(px), _round_half_away(py)
+        mask |= (rx >= 0) & (rx < w) & (ry >= 0) & (ry < h)
+    return (mask & inside).astype(np.float32)

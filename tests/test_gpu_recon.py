@@ -118,3 +118,34 @@ def test_training_with_the_proposal_in_the_bf16_form():
     assert last["loss"] < recs[0]["loss"] and math.isfinite(last["psnr"])
     assert last["judge_steps"] + last["proposal_steps"] + last["uniform_steps"] == last["step"]
     assert last["judge_steps"] >= 20  # the warm-up judges every step
+
+
+def test_density_volume_of_a_trained_field_matches_the_oracle(oracle):
+    """recon.density_volume (tree lookup + field + decoder on the GPU) of a
+    C1-shaped field after a few training steps, against the oracle's field
+    and decoder at the same voxel centres (node ids from the oracle's tree
+    lookup), FP64: relative L2 <= 1e-5, and the PSNR computed from it."""
+    from adaptivetensordf_b200 import recon
+    from adaptivetensordf_b200 import synthetic as syn
+
+    cfg = syn.CONFIGS["C1"]
+    small = syn.Config("C1-small", 32, 20, 11, 12.0, 32, cfg.tree_depth, cfg.channels, cfg.grid, cfg.hidden,
+                       1024, 16)
+    data = recon.make_tilt_series(small)
+    tree, geo = recon.build_model(small, "fp32", init_scale=0.05)
+    opt = recon.TrainOptions(epochs=2, batch=1024, max_samples_per_node=16)
+    recon.fit(tree, geo, data, opt)
+    N = small.volume
+    vol = recon.density_volume(tree, geo, N).cpu().numpy()
+    td, fd, md = syn.tree_dict(tree), syn.field_dict(geo, tree), syn.mlp_dict(geo)
+    pts = recon.voxel_centres(N, 0, N, "cpu").numpy()
+    node, _ = oracle.node_id_for_position(td, pts)
+    feat = oracle.vm_features(fd, td, pts, node, np.float64)
+    ref = oracle.mlp_forward(md, feat, np.float64).reshape(N, N, N)
+    assert float(np.abs(ref).max()) > 1e-3  # a nonzero field
+    err = np.linalg.norm(vol - ref) / np.linalg.norm(ref)
+    assert err < 1e-5, err
+    ph = data.volume.cpu().numpy().astype(np.float64)
+    m = ph.max()
+    p_ref = 10 * math.log10(1.0 / float((((ref - ph) / m) ** 2).mean()))
+    assert abs(recon.psnr(tree, geo, data.volume) - p_ref) < 1e-3

@@ -75,3 +75,33 @@ def test_refinement_inside_training_keeps_budget():
     refined = [r for r in logs if "refined_epoch" in r]
     assert refined and refined[0]["leaves"] <= 36 and refined[0]["leaves"] > 8
     assert np.isfinite(recs[-1]["psnr"]) and recs[-1]["psnr"] > recs[0]["psnr"] - 1.0
+
+
+def test_max_density_on_the_masked_corner_grid(oracle):
+    """compute_max_density: the 20^3 corner-to-corner grid of every leaf
+    (UniformGlobalSamples), each point masked by the tilt series' visibility
+    (PointInAnyImage), the maximum of the decoded density; against the
+    oracle's field and decoder at the same points and the numpy visibility
+    mask."""
+    from adaptivetensordf_b200 import recon
+    from adaptivetensordf_b200 import synthetic as syn
+    from oracle import scene_oracle as so
+
+    cfg = syn.Config("small", 32, 12, 7, 20.0, 24, 2, 8, 9, [32], 1024, 8)
+    data = recon.make_tilt_series(cfg)
+    tree, geo = recon.build_model(cfg, "fp32", init_scale=0.3)
+    recon.compute_max_density(tree, geo, data)
+    got = tree.node_max_density[tree.active_node_ids].cpu().numpy()
+    ids = tree.active_node_ids
+    pts = recon.uniform_global_samples(tree, ids, 20)
+    P = pts.reshape(-1, 3).cpu().numpy()
+    # the corner grid: first and last points are the leaf's corners
+    assert torch.equal(pts[:, 0], tree.node_position_min[ids]) and torch.equal(pts[:, -1], tree.node_position_max[ids])
+    node = ids[:, None].expand(-1, 8000).reshape(-1).cpu().numpy()
+    td, fd, md = syn.tree_dict(tree), syn.field_dict(geo, tree), syn.mlp_dict(geo)
+    dens = oracle.mlp_forward(md, oracle.vm_features(fd, td, P, node, np.float64), np.float64).reshape(-1)
+    mask = so.point_in_any_image(P, data.cam_rotation, None, data.cam_intrinsics, data.width, data.height, 1,
+                                 data.roi_min, data.roi_max)
+    assert 0.0 < mask.mean() < 1.0  # the corners of the volume are outside the +-60 deg field of view
+    ref = (dens * mask).reshape(len(ids), -1).max(1)
+    assert np.abs(got - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max())

@@ -92,3 +92,46 @@ def test_scene_directory_to_tilt_series(tmp_path):
     recs, reached = recon.train(cfg, "fp32", data, opt)
     assert reached is None and recs[-1]["psnr"] is None
     assert recs[-1]["loss"] < recs[0]["loss"]
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_point_in_any_image_matches_oracle(model):
+    """atdf_point_in_any_image (SceneBase::PointInAnyImage) bit for bit
+    against the numpy restatement: points in and out of the ROI, some exactly
+    on its bounds, on several orthographic tilts / pinhole poses."""
+    import ctypes as ct
+
+    from adaptivetensordf_b200 import capi
+    from oracle import scene_oracle as so
+
+    rng = np.random.default_rng(model + 3)
+    P = 50000
+    pts = rng.uniform(-1.3, 1.3, (P, 3)).astype(np.float32)
+    pts[:100, 0] = 1.0  # on the ROI bound (closed)
+    pts[100:200, 2] = -1.0
+    angles = np.linspace(-60, 60, 9)
+    rot = np.stack([so.tilt_quaternion(a) for a in angles])
+    if model == 1:
+        trans = None
+        K = np.array([24.0, 24.0, 23.5, 23.5, 0.3])
+        w = h = 48
+    else:
+        trans = np.stack([-3.0 * so.rotate(q[None], np.array([[0.0, 0.0, 1.0]]))[0] for q in rot])
+        K = np.array([40.0, 40.0, 31.5, 31.5, 0.0])
+        w, h = 64, 64
+    roi_min, roi_max = (-1.0, -0.9, -1.0), (1.0, 0.9, 1.0)
+    ref = so.point_in_any_image(pts, rot, trans, K, w, h, model, roi_min, roi_max)
+    pt = torch.from_numpy(pts).cuda()
+    rt = torch.from_numpy(rot).cuda()
+    tt = None if trans is None else torch.from_numpy(trans).cuda()
+    Kt = torch.from_numpy(K).cuda()
+    mask = torch.full((P,), -1.0, device="cuda")
+    L = capi.lib()
+    st = L.atdf_point_in_any_image(P, capi.ptr(pt), capi.ptr(rt), capi.ptr(tt), len(rot), capi.ptr(Kt), w, h, model,
+                                   (ct.c_float * 3)(*roi_min), (ct.c_float * 3)(*roi_max), capi.ptr(mask),
+                                   ct.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0
+    got = mask.cpu().numpy()
+    assert np.array_equal(got, ref)
+    assert 0.05 < ref.mean() < 0.95  # both outcomes occur
+    assert ref[:100].max() == 1.0  # points on the closed ROI bound can count

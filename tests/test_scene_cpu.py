@@ -106,3 +106,26 @@ def test_oracle_pinhole_direction_is_unit_and_origin_is_the_pose():
     qi = q[img] * np.array([-1, -1, -1, 1.0])  # inverse rotation
     np.testing.assert_allclose(so.rotate(qi, d.astype(np.float64)), cam, atol=2e-6)
     assert math.isclose(float(np.abs(so.tilt_quaternion(90.0)[1])), math.sin(math.pi / 4))
+
+
+def test_tilt_quaternions_reproduce_the_parallel_beam():
+    """recon.tilt_quaternions (with the off-axis rotation) rotate (0, 0, 1) to
+    the synthetic rays' direction and (u, v, 0) to their detector point."""
+    import math
+
+    from adaptivetensordf_b200 import recon
+    from adaptivetensordf_b200 import synthetic as syn
+    from oracle import scene_oracle as so
+
+    angles = np.array([-60.0, -13.5, 0.0, 42.0])
+    for off in (0.0, -3.7):
+        q = recon.tilt_quaternions(angles, off)
+        n = 16
+        img = np.repeat(np.arange(len(angles)), 3)
+        pix = np.tile([0, 37, 255], len(angles))
+        o, d = syn.parallel_beam_rays(angles, n, img, pix, off)
+        dq = so.rotate(q[img], np.tile([0.0, 0.0, 1.0], (len(img), 1)))
+        u = (pix % n + 0.5) / n * 2 - 1
+        v = (pix // n + 0.5) / n * 2 - 1
+        pq = so.rotate(q[img], np.stack([u, v, np.zeros_like(u)], 1)) - math.sqrt(2.0) * dq
+        assert np.abs(dq - d).max() < 1e-6 and np.abs(pq - o).max() < 1e-6
