@@ -12,8 +12,10 @@ form and the chosen BF16 form, with the seconds to a PSNR target.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0). Under torchrun each rank trains on its own ray
-batches and the gradients are all-reduced once per step (ray data
-parallelism; weak scaling). `--impl reference` times the CPU restatement of
+batches (ray data parallelism; weak scaling): the BF16 form's gradients are
+reduce-scattered, each rank updates its shard of the parameters and the BF16
+working copies are all-gathered (dp.ShardedAdam); the plain FP32 form
+all-reduces its gradients. `--impl reference` times the CPU restatement of
 the reference path (the reference itself has no CPU path and cannot be built
 here) on all host cores, on the headline workload.
 """
@@ -495,18 +497,32 @@ def measure_form(args, tree, cfg, form, dev_batches, host_batches, world, sample
     # the BF16 form's Adam also writes the BF16 working copies, on a side
     # stream so that the next step's segment pass overlaps it; the plain
     # FP32 form keeps torch's fused Adam
-    opt = Adam(params, lr=1e-3, geometry=geo, stream=torch.cuda.Stream()) if bf16 else \
-        torch.optim.Adam(params, lr=1e-3, fused=True)
-    join = opt.wait if bf16 else (lambda: None)  # the timed region ends after the last update
+    sharded = bf16 and world > 1
+    if sharded:
+        # ray data parallelism with the sharded step: reduce-scatter of the
+        # gradients, Adam on this rank's shard, all-gather of the BF16 copies
+        twins = list(geo.planes_bf16) + list(geo.lines_bf16)
+        opt = dp.ShardedAdam(params, world, int(os.environ.get("RANK", "0")), lr=1e-3,
+                             working={i: twins[i] for i in range(6)})
+        join = lambda: None  # noqa: E731
+    else:
+        opt = Adam(params, lr=1e-3, geometry=geo, stream=torch.cuda.Stream()) if bf16 else \
+            torch.optim.Adam(params, lr=1e-3, fused=True)
+        join = opt.wait if bf16 else (lambda: None)  # the timed region ends after the last update
 
     def step(o, d, y, k):
         rays = ab.RayList(o, d)
         img = geo.ProjectRays(tree, rays, M, 1 + k)
         loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
         img.backward(gimg)
-        dp.allreduce_gradients(params, world)
-        opt.step()
-        opt.zero_grad(set_to_none=True)
+        if sharded:
+            opt.step()
+            for p in params:
+                p.grad = None
+        else:
+            dp.allreduce_gradients(params, world)
+            opt.step()
+            opt.zero_grad(set_to_none=True)
         return loss
 
     for k in range(args.warmup):
