@@ -189,7 +189,7 @@ def _declare(L):
         "atdf_proposal_mlp_backward_bf16": (I32, [ct.POINTER(Mlp), ct.POINTER(Segments), P, P, ct.POINTER(MlpGrad), P,
                                                   P]),
         "atdf_proposal_allocate": (I32, [ct.POINTER(Segments), I64, P, I32, F32, F32, P]),
-        "atdf_proposal_samples": (I32, [ct.POINTER(Segments), P, F32, F32, U64, P, P, I64, P, P]),
+        "atdf_proposal_samples": (I32, [ct.POINTER(Segments), P, F32, F32, U64, I32, P, P, I64, P, P]),
         "atdf_proposal_loss": (I32, [ct.POINTER(Segments), P, P, P, F32, P, P, P, P, I64, P, P]),
         "atdf_proposal_occupancy": (I32, [P, P, I64, P, P]),
         "atdf_adam_step": (I32, [I64, P, P, P, P, P, F32, F32, F32, F32, F32, I64, P]),

@@ -436,6 +436,7 @@ constexpr int kSampThreads = 256;
 __global__ void __launch_bounds__(kSampThreads) proposal_samples_kernel(atdf_segments_t segs,
                                                                         const float* __restrict__ logits,
                                                                         float bin_mix, float bin_power, uint64_t seed,
+                                                                        int weight_rule,
                                                                         float* __restrict__ sample_t,
                                                                         float* __restrict__ sample_w, int64_t capacity,
                                                                         int32_t* err)
@@ -474,6 +475,18 @@ __global__ void __launch_bounds__(kSampThreads) proposal_samples_kernel(atdf_seg
             const float t = t0 + ((float)bcur + frac) * binw;
             return fminf(fmaxf(t, t0), t1);
         };
+        if (weight_rule == ATDF_PROPOSAL_WEIGHTS_IMPORTANCE) {
+            // importance weights: sample j stands for probability 1 / n of q,
+            // whose density in its bin b is p_b / binw, so w = binw / (n p_b)
+            // and sum_j w_j rho(t_j) estimates the segment integral without
+            // bias when the jitter is uniform
+            const float inv_n = 1.0f / (float)n;
+            for (int j = 0; j < n; ++j) {
+                sample_t[base + j] = place(j);
+                sample_w[base + j] = binw * inv_n / p[bcur * kSampThreads];
+            }
+            continue;
+        }
         // weights: the Voronoi cells of the placed samples within the segment,
         // the rule the uniform sampler applies to its own samples
         float t_prev = 0.0f, t_cur = place(0);
@@ -694,14 +707,15 @@ int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, co
 }
 
 int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, float bin_power,
-                          uint64_t seed, float* sample_t, float* sample_w, int64_t sample_capacity,
-                          int32_t* dev_error, atdf_stream_t stream)
+                          uint64_t seed, int32_t weight_rule, float* sample_t, float* sample_w,
+                          int64_t sample_capacity, int32_t* dev_error, atdf_stream_t stream)
 {
     if (!segments || !logits || !sample_t || !sample_w || sample_capacity < 0 ||
-        !(bin_mix > 0.0f && bin_mix <= 1.0f) || !(bin_power >= 0.0f && bin_power <= 1.0f))
+        !(bin_mix > 0.0f && bin_mix <= 1.0f) || !(bin_power >= 0.0f && bin_power <= 1.0f) ||
+        (weight_rule != ATDF_PROPOSAL_WEIGHTS_VORONOI && weight_rule != ATDF_PROPOSAL_WEIGHTS_IMPORTANCE))
         return ATDF_ERR_INVALID_ARGUMENT;
     proposal_samples_kernel<<<seg_blocks(segments->capacity), kSampThreads, 0, (cudaStream_t)stream>>>(
-        *segments, logits, bin_mix, bin_power, seed, sample_t, sample_w, sample_capacity, dev_error);
+        *segments, logits, bin_mix, bin_power, seed, weight_rule, sample_t, sample_w, sample_capacity, dev_error);
     ATDF_LAUNCH_CHECK();
     return ATDF_OK;
 }

@@ -163,8 +163,10 @@ struct GeometryTensorQO {
 // entry and exit points, the relative length, the leaf's occupancy as a whole
 // and per octant) to a 32-bin sample density over the segment and the
 // segment's mass; each ray's budget of samples is split by predicted mass and
-// drawn by stratified inverse-CDF sampling with weights 1 / (n q), so
-// projections stay unbiased. The network trains online on the bins of rho * w
+// drawn by stratified inverse-CDF sampling, weighted by the samples' Voronoi
+// cells (the uniform sampler's quadrature) or, with importance_weights, by
+// 1 / (n q) (an unbiased estimate of each segment's integral under uniform
+// jitter). The network trains online on the bins of rho * w
 // of uniform passes (ProjectUniformBinned), which also judge it. No call
 // reads device memory back to the host unless check_errors is set.
 class ProposalSampler {
@@ -189,6 +191,7 @@ class ProposalSampler {
     double mass_mix = 0.25, bin_mix = 0.2, mass_weight = 0.1;
     double mass_power = 0.5, bin_power = 0.5;  // sample density ~ predicted density^power
     bool check_errors = false;  // read the device error words after each call (synchronises)
+    bool importance_weights = false;  // sample weights 1 / (n q) instead of Voronoi cells
     // "fp32": the MLP on CUDA cores in FP32; "bf16": on the tensor cores
     // (tcgen05, BF16 operands), 3 hidden layers only
     std::string precision = "fp32";

@@ -150,6 +150,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
         .def_readwrite("mass_weight", &ProposalSampler::mass_weight)
         .def_readwrite("mass_power", &ProposalSampler::mass_power)
         .def_readwrite("bin_power", &ProposalSampler::bin_power)
+        .def_readwrite("importance_weights", &ProposalSampler::importance_weights)
         .def_readwrite("check_errors", &ProposalSampler::check_errors)
         .def_readwrite("precision", &ProposalSampler::precision);
 

@@ -914,7 +914,9 @@ Tensor ProposalSampler::Project(HyperTreeBase& tree, GeometryTensorQO& geo, cons
     auto xt = torch::empty({std::max<int64_t>(cap, 1)}, o.options());
     auto xw = torch::empty_like(xt);
     check_status(atdf_proposal_samples(&view, logits.data_ptr<float>(), (float)bin_mix, (float)bin_power,
-                                       jitter_seed, xt.data_ptr<float>(), xw.data_ptr<float>(), cap,
+                                       jitter_seed, importance_weights ? ATDF_PROPOSAL_WEIGHTS_IMPORTANCE
+                                                                       : ATDF_PROPOSAL_WEIGHTS_VORONOI,
+                                       xt.data_ptr<float>(), xw.data_ptr<float>(), cap,
                                        err.data_ptr<int32_t>(), stream_arg()),
                  "atdf_proposal_samples");
     ProjectArgs args{&geo, &tree, 0, 0, {}, ws, xt, xw};

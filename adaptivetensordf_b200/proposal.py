@@ -20,8 +20,12 @@ every judge_every_closed steps while it is closed (every step during the
 first `warmup` steps, to train the proposal). Only the gate's error is read
 back to the host, once per judge step after the warm-up.
 
-The proposal's samples follow a quadrature rule, not an unbiased estimator,
-so its error is a bias that the field learns to fit. With ``residual_gate``
+With the default Voronoi-cell weights the proposal's samples follow a
+quadrature rule, not an unbiased estimator, so its error is a bias that the
+field learns to fit. With ``importance=True`` the samples carry importance
+weights 1 / (n q) and the proposal density follows the predicted density
+(bin power 1): each projection is an unbiased estimate of the uniform one,
+and its error is noise of zero mean. With ``residual_gate``
 > 0 (and the batch's targets passed to ``project``) the gate also requires
 that error to stay small beside the current fit: ||proposal - judge|| <=
 residual_gate * ||judge - target||. Early in training the residual is large
@@ -40,7 +44,7 @@ class ProposalSchedule:
     def __init__(self, tree, geo, max_samples_per_node: int, budget: int = 64, judge_every: int = 10,
                  gate: float = 0.01, lr: float = 3e-3, warmup: int = 20, device: str = "cuda", seed: int = 1005,
                  jitter: bool = True, judge_every_closed: int = 4, sampler=None, residual_gate: float = 0.0,
-                 judge_every_retired: int = 100):
+                 judge_every_retired: int = 100, importance: bool = False):
         self.tree, self.geo = tree, geo
         self.M = max_samples_per_node
         if sampler is None:
@@ -49,6 +53,9 @@ class ProposalSchedule:
             sampler = ProposalSampler(tree.NumNodes(), 64, 3, seed, device)
         self.ps = sampler
         self.ps.budget = budget
+        if importance:
+            self.ps.importance_weights = True
+            self.ps.bin_power = 1.0
         # the BF16 form runs the proposal MLP on the tensor cores too (3 hidden layers)
         if getattr(geo, "precision", "fp32") == "bf16" and len(getattr(sampler, "weight", [])) == 4:
             self.ps.precision = "bf16"

@@ -363,6 +363,7 @@ class TrainOptions:
     judge_every: int = 10       # proposal: steps between judge passes while open
     residual_gate: float = 0.5   # proposal: its error must stay within this share of the fit residual (0: off)
     proposal_jitter: bool = True  # proposal: jittered (True) or midpoint stratum samples
+    proposal_importance: bool = False  # proposal: importance weights 1 / (n q) instead of Voronoi cells
     start_depth: int = 0        # active depth of the initial tree (0: the config's depth)
     refine_every: int = 0       # epochs between structure refinements (0: none)
     max_active_nodes: int = 0   # leaf budget of the refinement
@@ -462,7 +463,8 @@ def train(cfg, form: str, data: TiltSeries, opt: TrainOptions, log=None, device=
 
         prop = ProposalSchedule(tree, geo, opt.max_samples_per_node, budget=opt.budget, gate=opt.gate,
                                 residual_gate=opt.residual_gate,
-                                judge_every=opt.judge_every, device=device, jitter=opt.proposal_jitter)
+                                judge_every=opt.judge_every, device=device, jitter=opt.proposal_jitter,
+                                importance=opt.proposal_importance)
 
     n = data.num_rays
     steps_per_epoch = n // opt.batch
@@ -593,6 +595,7 @@ def main():
     ap.add_argument("--judge-every", type=int, default=10)
     ap.add_argument("--residual-gate", type=float, default=0.5)
     ap.add_argument("--no-prop-jitter", action="store_true")
+    ap.add_argument("--prop-importance", action="store_true", help="proposal samples with importance weights")
     ap.add_argument("--start-depth", type=int, default=0)
     ap.add_argument("--refine-every", type=int, default=0)
     ap.add_argument("--max-leaves", type=int, default=0)
@@ -622,7 +625,8 @@ def main():
                        lr_grid=a.lr_grid, lr_decoder=a.lr_decoder, lr_decay=a.lr_decay, loss_tv=a.tv,
                        init_scale=a.init_scale,
                        budget=a.budget, gate=a.gate, judge_every=a.judge_every, residual_gate=a.residual_gate,
-                       proposal_jitter=not a.no_prop_jitter, start_depth=a.start_depth,
+                       proposal_jitter=not a.no_prop_jitter, proposal_importance=a.prop_importance,
+                       start_depth=a.start_depth,
                        refine_every=a.refine_every, max_active_nodes=a.max_leaves, tone_mapper=a.tone_mapper)
     recs, reached = train(cfg, a.form, data, opt, log=lambda r: print(json.dumps(r), flush=True))
     print(json.dumps({"form": a.form, "config": a.config, "seconds_to_target": reached, "target": a.target,

@@ -402,12 +402,18 @@ int atdf_proposal_allocate(const atdf_segments_t* segments, int64_t num_rays, co
  * seed, 0.5 for seed 0) from q = (1 - bin_mix) softmax(bin_power * bin
  * logits) + bin_mix / 32 over 32 equal bins (the predicted distribution
  * raised to bin_power in [0, 1]; bin_mix in (0, 1] keeps samples
- * everywhere). Weights are the samples' Voronoi cells within the segment,
- * the rule of the uniform sampler (HyperTree.cu:495-512): with uniform q the
- * result is the uniform per-node quadrature with these counts. */
+ * everywhere). weight_rule ATDF_PROPOSAL_WEIGHTS_VORONOI: the samples'
+ * Voronoi cells within the segment, the rule of the uniform sampler
+ * (HyperTree.cu:495-512), so with uniform q the result is the uniform
+ * per-node quadrature with these counts; ATDF_PROPOSAL_WEIGHTS_IMPORTANCE:
+ * w_j = 1 / (n q(t_j)) (bin width / (n p_bin)), the importance weights under
+ * which sum_j w_j rho(t_j) is an unbiased estimate of the segment integral
+ * for uniform jitter. */
+#define ATDF_PROPOSAL_WEIGHTS_VORONOI 0
+#define ATDF_PROPOSAL_WEIGHTS_IMPORTANCE 1
 int atdf_proposal_samples(const atdf_segments_t* segments, const float* logits, float bin_mix, float bin_power,
-                          uint64_t seed, float* sample_t, float* sample_w, int64_t sample_capacity,
-                          int32_t* dev_error, atdf_stream_t stream);
+                          uint64_t seed, int32_t weight_rule, float* sample_t, float* sample_w,
+                          int64_t sample_capacity, int32_t* dev_error, atdf_stream_t stream);
 
 /* Training loss of the proposal against seg_bins of a uniform binned forward
  * on the same segments: mean over segments of the cross-entropy of the

@@ -93,12 +93,13 @@ def bin_probs(lg, bin_mix, power=1.0):
     return p * (1 - bin_mix) + bin_mix / BINS
 
 
-def samples(tmin, tmax, nsamp, logits, bin_mix, a=None, bin_power=1.0):
+def samples(tmin, tmax, nsamp, logits, bin_mix, a=None, bin_power=1.0, importance=False):
     """t and weight of every segment's samples, concatenated in segment
     order: u_j = (j + a_j) / n, inverse CDF of the binned density (the
     predicted one raised to bin_power, mixed with uniform); weights are the
-    Voronoi cells of the placed t within the segment. a: per-segment arrays
-    of jitter (None: 0.5)."""
+    Voronoi cells of the placed t within the segment, or with importance
+    the importance weights 1 / (n q(t_j)) = bin width / (n p_bin). a:
+    per-segment arrays of jitter (None: 0.5)."""
     ts, ws = [], []
     for s in range(len(nsamp)):
         n = int(nsamp[s])
@@ -106,7 +107,7 @@ def samples(tmin, tmax, nsamp, logits, bin_mix, a=None, bin_power=1.0):
         cdf = np.concatenate([[0.0], np.cumsum(p)])
         t0, t1 = float(tmin[s]), float(tmax[s])
         binw = (t1 - t0) / BINS
-        tt = []
+        tt, tb = [], []
         for j in range(n):
             aj = 0.5 if a is None else float(a[s][j])
             u = (j + aj) / n
@@ -114,6 +115,11 @@ def samples(tmin, tmax, nsamp, logits, bin_mix, a=None, bin_power=1.0):
             b = min(max(b, 0), BINS - 1)
             frac = min(max((u - cdf[b]) / p[b], 0.0), 1.0)
             tt.append(min(max(t0 + (b + frac) * binw, t0), t1))
+            tb.append(b)
+        if importance:
+            ts.extend(tt)
+            ws.extend(binw / (n * p[b]) for b in tb)
+            continue
         for j in range(n):
             lo = t0 if j == 0 else 0.5 * (tt[j - 1] + tt[j])
             hi = t1 if j == n - 1 else 0.5 * (tt[j + 1] + tt[j])

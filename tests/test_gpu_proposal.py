@@ -166,7 +166,7 @@ def test_placed_arbitrary_samples_match_oracle(oracle):
     S = int(pl.totals()[1])
     xt = torch.empty(S, device="cuda")
     xw = torch.empty(S, device="cuda")
-    assert L.atdf_proposal_samples(ct.byref(pl.view), c.ptr(logits), ct.c_float(0.2), ct.c_float(1.0), 99,
+    assert L.atdf_proposal_samples(ct.byref(pl.view), c.ptr(logits), ct.c_float(0.2), ct.c_float(1.0), 99, 0,
                                    c.ptr(xt), c.ptr(xw), S, c.ptr(pl.err), None) == 0
     torch.cuda.synchronize()
     assert int(pl.err.item()) == 0
@@ -249,17 +249,17 @@ def test_proposal_kernels_match_restatement(oracle):
     assert np.all(b["n"] >= 1)
     S = int(pl.totals()[1])
     assert S == int(b["ray_sample_offset"][-1])
-    for seed in (0, 4242):
+    for seed, rule in ((0, 0), (4242, 0), (4242, 1)):
         xt = torch.empty(S, device="cuda")
         xw = torch.empty(S, device="cuda")
         assert L.atdf_proposal_samples(ct.byref(pl.view), c.ptr(logits), ct.c_float(0.2), ct.c_float(0.5), seed,
-                                       c.ptr(xt), c.ptr(xw), S, c.ptr(pl.err), None) == 0
+                                       rule, c.ptr(xt), c.ptr(xw), S, c.ptr(pl.err), None) == 0
         torch.cuda.synchronize()
         jit = None
         if seed:
             jit = [[oracle.jitter(seed, int(b["ray"][s]), int(b["node"][s]), j) for j in range(int(b["n"][s]))]
                    for s in range(G)]
-        t_ref, w_ref = po.samples(b["tmin"], b["tmax"], b["n"], lg, 0.2, jit, bin_power=0.5)
+        t_ref, w_ref = po.samples(b["tmin"], b["tmax"], b["n"], lg, 0.2, jit, bin_power=0.5, importance=rule == 1)
         t = xt.cpu().numpy()
         w = xw.cpu().numpy()
         ln = np.repeat(b["tmax"] - b["tmin"], b["n"])

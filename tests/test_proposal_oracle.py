@@ -85,3 +85,36 @@ def test_octant_sums_split_each_segment():
     assert nm[3, 8] == 32 and abs(nl[3, 8] - 2.0) < 1e-12
     assert nm[3, 4] == 16 and nm[3, 5] == 16  # (x<=0, y<0, z>0) and (x>0, y<0, z>0)
     assert abs(nl[3, :8].sum() - 2.0) < 1e-12
+
+
+def test_importance_weights_are_unbiased():
+    """With importance weights 1 / (n q(t)) and uniform jitter, the weighted
+    sum of a density along a segment averages to its integral (for any
+    proposal q with full support), while the Voronoi-cell weights of the
+    same samples keep a bias when q is far from the density."""
+    from oracle import proposal_oracle as po
+
+    rng = np.random.default_rng(5)
+    t0, t1, n = 0.3, 1.7, 6
+
+    def rho(t):
+        return np.where(t < 0.9, 0.05, 1.0 + 0.5 * np.sin(7 * t))
+
+    grid = np.linspace(t0, t1, 200001)
+    exact = np.trapezoid(rho(grid), grid)
+    logits = rng.normal(0, 2.0, (1, po.BINS + 1))  # a poor proposal
+    est_i, est_v = [], []
+    for k in range(4000):
+        a = [rng.random(n)]
+        t, w = po.samples(np.array([t0]), np.array([t1]), np.array([n]), logits, 0.2, a, 1.0, importance=True)
+        est_i.append((w * rho(t)).sum())
+        t, w = po.samples(np.array([t0]), np.array([t1]), np.array([n]), logits, 0.2, a, 1.0, importance=False)
+        est_v.append((w * rho(t)).sum())
+    mi, se = np.mean(est_i), np.std(est_i) / np.sqrt(len(est_i))
+    assert abs(mi - exact) < 4 * se + 1e-9, (mi, exact, se)
+    # with a uniform proposal both rules place the same samples and weights
+    flat = np.zeros((1, po.BINS + 1))
+    t, wi = po.samples(np.array([t0]), np.array([t1]), np.array([n]), flat, 0.2, None, 1.0, importance=True)
+    _, wv = po.samples(np.array([t0]), np.array([t1]), np.array([n]), flat, 0.2, None, 1.0, importance=False)
+    assert np.allclose(wi, (t1 - t0) / n) and np.allclose(wv, (t1 - t0) / n)
+    assert abs(np.mean(est_v) - exact) > 4 * np.std(est_v) / np.sqrt(len(est_v))  # the Voronoi rule is biased
