@@ -750,7 +750,66 @@ def run_ours(args, rank, world):
     if not args.no_cpu_baseline:
         t = oracle_tree(cfg)
         line["cpu_baseline"] = cpu_baseline(cfg, t, args.cpu_rays, 3)
+        # the FP64 oracle as the checker of the BF16 form's error (C3 asks
+        # for it; the C5 shapes beside it)
+        line["bf16_err_vs_fp64"] = {"C3": bf16_error_vs_oracle(workload_config("C3")),
+                                    "C5": bf16_error_vs_oracle(cfg)}
     print(json.dumps(line), flush=True)
+
+
+def bf16_error_vs_oracle(cfg, R=256, seed=4321):
+    """Relative L2 error of the BF16 form's projection and gradients (the
+    tensor-core kernels) against the FP64 oracle on the same samples of R
+    rays of the workload: `vs_bf16_params` with the oracle on the
+    BF16-rounded factors and weights (the decoder's BF16 arithmetic alone),
+    `vs_fp32_params` with the FP32 parameters (what the precision form costs
+    in total)."""
+    import torch
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+    from oracle import oracle as O
+
+    if cfg.target_leaves:
+        tree = syn.adaptive_tree(cfg, syn.config_phantom(cfg, 1001), device="cuda")
+    else:
+        tree = syn.make_tree(cfg.tree_depth, device="cuda")
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    o, d = syn.random_ray_batch(cfg, R, seed)
+    M = cfg.max_samples_per_node
+    img = geo.ProjectRays(tree, ab.RayList(torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()), M, seed)
+    gi = np.random.default_rng(seed).normal(size=(1, R))
+    img.backward(torch.from_numpy(gi.astype(np.float32)).cuda())
+    geo.CheckErrors()
+    td, fd, md = syn.tree_dict(tree), syn.field_dict(geo, tree), syn.mlp_dict(geo)
+
+    def bf(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(torch.bfloat16).to(torch.float64).numpy()
+
+    fd_b = {**fd, "planes": [bf(p) for p in fd["planes"]], "lines": [bf(x) for x in fd["lines"]]}
+    md_b = {**md, "layers": [(bf(w), b.astype(np.float64)) for w, b in md["layers"]]}
+    md_b["layers"][-1] = (md["layers"][-1][0].astype(np.float64), md["layers"][-1][1].astype(np.float64))
+    segs = O.ray_segments(td, o, d, M)
+    so = O.emit_samples(segs, o, d, O.jitter_for_segments(seed, segs))
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+    out = {"rays": R, "samples": int(segs["n"].sum())}
+    for name, f_, m_ in (("vs_bf16_params", fd_b, md_b), ("vs_fp32_params", fd, md)):
+        ref = O.project_forward(f_, m_, td, so, R, np.float64)
+        g = O.project_backward(f_, m_, td, so, R, gi, np.float64)
+        pg = np.concatenate([geo.planes[k].grad.cpu().numpy().ravel() for k in range(3)])
+        pr = np.concatenate([g["planes"][k].ravel() for k in range(3)])
+        lg = np.concatenate([geo.lines[k].grad.cpu().numpy().ravel() for k in range(3)])
+        lr = np.concatenate([g["lines"][k].ravel() for k in range(3)])
+        dg = np.concatenate([x.grad.cpu().numpy().ravel() for x in list(geo.decoder_weight) + list(geo.decoder_bias)])
+        dr = np.concatenate([x.ravel() for x in list(g["W"]) + list(g["b"])])
+        out[name] = {"image": rel(img.detach().cpu().numpy(), ref), "plane_grad": rel(pg, pr),
+                     "line_grad": rel(lg, lr), "decoder_grad": rel(dg, dr)}
+    return out
 
 
 def make_host_shapes(R):

@@ -28,10 +28,12 @@ from tests.scene import rel_err
 pytestmark = pytest.mark.gpu
 
 REL_TOL = 1e-5
-# BF16 form against the FP64 oracle on the BF16-rounded parameters: the image
-# carries the BF16 rounding of the decoder's activations (measured 2-4e-5),
-# the gradients also that of the backward's operands (measured 2-4e-3)
-BF16_TOL = {"image": 2e-4, "plane": 1e-2, "line": 1e-2, "W": 1e-2, "b": 1e-2}
+# BF16 form against the FP64 oracle on the BF16-rounded parameters, about
+# three times the measured errors (M = 24 / 96): the image carries the BF16
+# rounding of the decoder's activations (1.4e-5 / 7e-6), the plane and line
+# gradients also that of the backward's operands (1.9e-3 / 2.9e-3), the
+# first-layer weights 2e-3, the other decoder parameters <= 1.4e-4
+BF16_TOL = {"image": 5e-5, "plane": 6e-3, "line": 9e-3, "W": 6e-3, "b": 5e-4}
 
 
 @pytest.fixture(scope="module", autouse=True)
