@@ -226,7 +226,8 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
 
 // Takes the next work item; fills the segment table; issues the plane TMA
 // when the item starts a new slot. Returns the item's slot, or -1 when the
-// queue is empty.
+// queue is empty. Items of up to map_cap (<= kSegMapCap) samples get the
+// sample -> segment byte map, larger ones a binary search.
 // A work item's samples are visited in the order k -> k * 104729 mod total
 // (a permutation: the prime exceeds any item's sample count). Consecutive
 // samples, which share a warp, then come from different rays and depths in
@@ -276,7 +277,7 @@ __device__ __forceinline__ void init_item_queue(int* s_ctl)
 }
 
 __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, float* sm, SegTab tab, uint64_t* bar,
-                                              int* s_ctl, bool want_dI)
+                                              int* s_ctl, bool want_dI, int map_cap = kSegMapCap)
 {
     const Ws& w = p.ws;
     const int tid = threadIdx.x;
@@ -426,7 +427,7 @@ __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, f
     info.inv_total = info.total > 0 ? 1.0 / (double)info.total : 0.0;
     // sample -> segment map (one byte per sample), in place of a binary
     // search of the count scan per sample
-    info.use_map = info.total <= kSegMapCap;
+    info.use_map = info.total <= map_cap;
     if (info.use_map && tid < info.nseg) {
         const int b = tab.start[tid], e = tab.start[tid + 1];
         for (int k = b; k < e; ++k) tab.map[k] = (unsigned char)tid;

@@ -14,11 +14,12 @@
 //     exact zeros, so the result equals the 24-channel product.
 //   * The backward keeps the slot's planes (41.6 KB) and their fixed-point
 //     gradient copy (83 KB) in shared memory, which leaves room for one
-//     128-row tile at a time: one half of 256 threads, two per sample row.
-//     Thread group g of a row owns 12 channels, [8g, 8g + 8) and
-//     [16 + 4g, 16 + 4g + 4) (one 16-byte and one 8-byte piece of a 48-byte
-//     texel), and scatters them to all four bilinear corners itself, so no
-//     per-row scratch is shared between the two threads.
+//     128-row tile at a time, with three threads per sample row (384
+//     threads). Thread group g of a row owns the 8 channels [8g, 8g + 8) (one
+//     16-byte piece of a 48-byte texel) in the feature gather and scatters
+//     them to all four bilinear corners itself, so no per-row scratch is
+//     shared between the threads; groups 0 and 1 also own the hidden columns
+//     [32g, 32g + 32) of the decoder's epilogues, while group 2 waits.
 // The line-gradient MMA has N = 72 columns padded to 80 (the columns past 72
 // of its output are not read).
 
@@ -54,8 +55,14 @@ constexpr int kLineWin = 32;     // line-gradient window entries per line (share
 constexpr int kLineRows = 21;    // rows per line in the line-gradient MMA (3 lines <= 64 rows)
 constexpr int kLineN = 80;       // N of the line-gradient MMA (3 * 24 = 72, padded)
 constexpr int kThreadsF = 256;   // forward: two halves of 128 rows, one thread per row
-constexpr int kThreadsB = 256;   // backward: one half of 128 rows, two threads per row
-constexpr uint32_t kTmemF = 256;  // columns per forward CTA
+constexpr int kThreadsB = 384;   // backward: one half of 128 rows, three threads per row
+// The shared fixed-point gradient keeps each texel's 24 channels at a pitch
+// of 25 words: texel * 24 mod 32 takes only 4 values, so the atomics of a
+// warp (random texels, one channel) would meet in 4 banks; with an odd pitch
+// they spread over all 32.
+constexpr int kGP = 25;
+constexpr int kMapCapF = 2048;    // forward: items of up to this many samples use the byte map
+constexpr uint32_t kTmemF = 256;  // columns per forward CTA (two CTAs per SM)
 constexpr uint32_t kTmemB = 512;  // columns per backward CTA (one CTA per SM)
 
 __device__ __forceinline__ uint32_t hb_off(int s, int c) { return tc::mnmajor_off(c, s, kHBCols); }
@@ -65,6 +72,7 @@ __device__ __forceinline__ uint32_t w1_off(int n, int k) { return tc::kmajor_off
 
 struct Smem24 {
     uint32_t planes, w0, w1, bias, hb[2], g, gplanes, gline, segi, total;
+    // gplane_elems: the unpadded plane-gradient elements (texels x 24)
     __host__ __device__ Smem24(int plane_elems, int gplane_elems, bool bwd)
     {
         auto al = [](uint32_t x) { return (x + 127u) & ~127u; };
@@ -84,51 +92,16 @@ struct Smem24 {
         g = o;
         if (bwd) o = al(o + kRows * kGCols * 2);
         gplanes = o;
-        if (bwd) o = al(o + gplane_elems * 4);
+        if (bwd) o = al(o + ((gplane_elems / kC * kGP + 3) & ~3) * 4);
         gline = o;
         if (bwd) o = al(o + 3 * kLineWin * kC * 4);
         segi = o;
-        o = al(o + kSegTabFloats * 4);
+        // the forward's table keeps a sample -> segment map of kMapCapF
+        // samples only, which lets two forward CTAs share an SM
+        o = al(o + (bwd ? kSegTabFloats : kSegTabFloats - (kSegMapCap - kMapCapF) / 4) * 4);
         total = o;
     }
 };
-
-// 8 BF16 in an 8-byte piece -> 4 floats.
-__device__ __forceinline__ void unpack_bf16x4(const uint2& u, float* f)
-{
-    const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const float2 x = __bfloat1622float2(p[i]);
-        f[2 * i] = x.x;
-        f[2 * i + 1] = x.y;
-    }
-}
-
-__device__ __forceinline__ void store_bf16x4(unsigned char* dst, const float* v)
-{
-    uint2 u;
-    u.x = pack_bf16(v[0], v[1]);
-    u.y = pack_bf16(v[2], v[3]);
-    *reinterpret_cast<uint2*>(dst) = u;
-}
-
-// The 12 channels of group g of a 48-byte BF16 texel: [8g, 8g+8) into
-// v[0..7], [16+4g, 16+4g+4) into v[8..11].
-__device__ __forceinline__ void load12(const unsigned char* tx, int g, float (&v)[12])
-{
-    unpack_bf16x8(*reinterpret_cast<const uint4*>(tx + 16 * g), v);
-    unpack_bf16x4(*reinterpret_cast<const uint2*>(tx + 32 + 8 * g), v + 8);
-}
-
-__device__ __forceinline__ void load12_global(const unsigned char* tx, int g, float (&v)[12])
-{
-    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(tx + 16 * g)), v);
-    unpack_bf16x4(__ldg(reinterpret_cast<const uint2*>(tx + 32 + 8 * g)), v + 8);
-}
-
-// Channel of entry i (0..11) of group g.
-__device__ __forceinline__ int chan12(int g, int i) { return i < 8 ? 8 * g + i : 16 + 4 * g + (i - 8); }
 
 __device__ __forceinline__ void load_weights(const FusedParams& p, unsigned char* sm, const Smem24& L)
 {
@@ -229,7 +202,7 @@ __device__ __forceinline__ void gather24(const FusedParams& p, const unsigned ch
     }
 }
 
-__global__ void __launch_bounds__(kThreadsF, 1) tc24_forward_kernel(FusedParams p)
+__global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams p)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar_tma;
@@ -262,7 +235,7 @@ __global__ void __launch_bounds__(kThreadsF, 1) tc24_forward_kernel(FusedParams 
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true;
     while (alive) {
-        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false);
+        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false, kMapCapF);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {
@@ -356,65 +329,42 @@ __global__ void __launch_bounds__(kThreadsF, 1) tc24_forward_kernel(FusedParams 
 // ---------------------------------------------------------------------------
 // backward: one half of 128 rows, two threads per row (group g = tid / 128)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void cta_barrier() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void cta_barrier() { asm volatile("bar.sync 1, 384;" ::: "memory"); }
 
-// Plane (bilinear) and line (linear) values of plane / line m for the 12
-// channels of group g of one sample.
-__device__ __forceinline__ void gather12(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
-                                         int grp, float (&mat)[12], float (&vec)[12])
+// Plane (bilinear) and line (linear) values of plane / line m for the 8
+// channels of group g (channels 8g .. 8g + 7) of one sample.
+__device__ __forceinline__ void gather8(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
+                                        int grp, float (&mat)[8], float (&vec)[8])
 {
     const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
     const int Wp = p.plane_pitch[m];
     const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
     const Corner1 l = corners1(g.lu[m], L);
-    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
+    const unsigned char* P = sm + (size_t)p.plane_off[m] * 2 + 16 * grp;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        float w, u[12];
-        load12(P + corner_texel(k, j, Wp, w) * (kC * 2), grp, u);
+        float w, u[8];
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(P + corner_texel(k, j, Wp, w) * (kC * 2)), u);
 #pragma unroll
-        for (int i = 0; i < 12; ++i) mat[i] = j == 0 ? u[i] * w : fmaf(u[i], w, mat[i]);
+        for (int i = 0; i < 8; ++i) mat[i] = j == 0 ? u[i] * w : fmaf(u[i], w, mat[i]);
     }
-    const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]);
-    float v0[12], v1[12];
-    load12_global(V + l.x0 * (kC * 2), grp, v0);
-    load12_global(V + l.x1 * (kC * 2), grp, v1);
+    const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]) + 16 * grp;
+    float v0[8], v1[8];
+    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x0 * (kC * 2))), v0);
+    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x1 * (kC * 2))), v1);
 #pragma unroll
-    for (int i = 0; i < 12; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
+    for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
 }
 
-__device__ __forceinline__ void line12(const FusedParams& p, const SampleGeo& g, int m, int grp, float (&vec)[12])
+__device__ __forceinline__ void line8(const FusedParams& p, const SampleGeo& g, int m, int grp, float (&vec)[8])
 {
     const Corner1 l = corners1(g.lu[m], p.field.line_len[m]);
-    const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]);
-    float v0[12], v1[12];
-    load12_global(V + l.x0 * (kC * 2), grp, v0);
-    load12_global(V + l.x1 * (kC * 2), grp, v1);
+    const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]) + 16 * grp;
+    float v0[8], v1[8];
+    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x0 * (kC * 2))), v0);
+    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x1 * (kC * 2))), v1);
 #pragma unroll
-    for (int i = 0; i < 12; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
-}
-
-// 12 values of group g into row t of the feature buffer at column base c0
-// (the group's channels of a 24-channel block): 8 at c0 + 8g, 4 at
-// c0 + 16 + 4g.
-__device__ __forceinline__ void store12(unsigned char* hb, int t, int c0, int grp, const float (&v)[12])
-{
-    store_bf16x8(hb + hb_off(t, c0 + 8 * grp), v);
-    store_bf16x4(hb + hb_off(t, c0 + 16 + 4 * grp), v + 8);
-}
-
-// 12 TMEM columns of this thread's row: 8 at col + 8g, 4 at col + 16 + 4g.
-__device__ __forceinline__ void tld12(uint32_t base, int col, int grp, float (&v)[12])
-{
-    float a[8];
-    uint32_t b[4];
-    tc::ld_32x32b_x8(trow(base, col + 8 * grp), a);
-    tc::ld_32x32b_x4(trow(base, col + 16 + 4 * grp), b);
-    tc::wait_ld();
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = a[i];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) v[8 + i] = __uint_as_float(b[i]);
+    for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
 }
 
 __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams p)
@@ -425,7 +375,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     __shared__ uint32_t s_tmem;
     __shared__ int s_ctl[8];
     __shared__ int s_lo[3];
-    __shared__ float s_z[2][kRows];  // partial last-layer sums [group][row]
+    __shared__ float s_z[2][kRows];  // partial last-layer sums [group 0 / 1][row]
     // fixed-point plane-gradient accumulation of the current slot
     __shared__ float s_tcum;    // sum of |contribution| over the slot's tiles so far
     __shared__ float s_tfirst;  // the same over its first tile (scale choice)
@@ -433,7 +383,8 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     __shared__ int s_fb;        // a tile of the slot went to global memory in FP32
     const Smem24 L(p.plane_off[3], p.gplane_off[3], true);
     const int tid = threadIdx.x, grp = tid >> 7, t = tid & (kRows - 1), lane = tid & 31;
-    const int col0 = 32 * grp;  // hidden columns of this group
+    const bool mlp = grp < 2;   // the group owns hidden columns
+    const int col0 = 32 * grp;  // hidden columns of groups 0 and 1
     const bool issuer = tid == 0;
     if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemB);
     if (tid == 0) {
@@ -450,21 +401,24 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     const uint32_t tbase = s_tmem;
     // TMEM: D0 / dX (0..63), D1 / dH0 (64..127), the line MMA over 0..79 once
     // both are consumed, the weight-gradient accumulator (128..223), and the
-    // BF16 plane values of the feature step (256 + 18 g .. 256 + 18 g + 17)
+    // BF16 plane values of the feature step (256 + 12 g .. 256 + 12 g + 11)
     const uint32_t d0 = tbase, d1 = tbase + 64, dacc = tbase + 128;
-    const uint32_t stash = tbase + 256 + 18 * grp;
+    const uint32_t stash = tbase + 256 + 12 * grp;
     SegTab tab = seg_tab(reinterpret_cast<float*>(sm + L.segi));
     const float* bias = reinterpret_cast<const float*>(sm + L.bias);
     const float beta = p.mlp.softplus_beta;
     const int lact = p.mlp.last_activation;
-    const int gplane_elems = p.gplane_off[3];
+    // the slot's plane gradients in shared memory: plane m's texels from
+    // gpo[m], kGP words each
+    const int gpl_words = (p.gplane_off[3] / kC * kGP + 3) & ~3;
+    const int gpo[3] = {p.gplane_off[0] / kC * kGP, p.gplane_off[1] / kC * kGP, p.gplane_off[2] / kC * kGP};
     int* gpl = reinterpret_cast<int*>(sm + L.gplanes);
     float* gln = reinterpret_cast<float*>(sm + L.gline);
     unsigned char* hb = sm + L.hb[0];
     unsigned char* gb = sm + L.g;
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true, had_tile = false;
-    float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group
+    float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group (groups 0, 1)
     float scale = 0.f;           // the slot's fixed-point scale
     int ntiles = 0;              // tiles of the slot
     while (alive) {
@@ -472,7 +426,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {
-            for (int i = tid * 4; i < gplane_elems; i += kThreadsB * 4)
+            for (int i = tid * 4; i < gpl_words; i += kThreadsB * 4)
                 *reinterpret_cast<int4*>(gpl + i) = make_int4(0, 0, 0, 0);
             // the slot's global gradient starts at zero (the caller does not
             // clear it): a tile that overflows the fixed-point range adds to it
@@ -517,18 +471,18 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             const bool handshake = !scale_set && t0 == 0;
             const int k = t0 + t;
             const bool valid = k < it.total;
-            // features (own 12 channels), plane values kept as BF16 in TMEM
+            // features (own 8 channels), plane values kept as BF16 in TMEM
             SampleGeo g;
             float w = 0.0f;
             int si = -1;
-            float f[12];
-            uint32_t pk[3][6];
+            float f[8];
+            uint32_t pk[3][4];
 #pragma unroll
-            for (int i = 0; i < 12; ++i) f[i] = 0.0f;
+            for (int i = 0; i < 8; ++i) f[i] = 0.0f;
 #pragma unroll
             for (int m = 0; m < 3; ++m)
 #pragma unroll
-                for (int i = 0; i < 6; ++i) pk[m][i] = 0u;
+                for (int i = 0; i < 4; ++i) pk[m][i] = 0u;
             if (valid) {
                 const SampleState st = sample_state(p, tab, it, k);
                 w = st.w;
@@ -537,23 +491,18 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     g = sample_geo_fast(p, tab, st.node, st.pos);
 #pragma unroll
                     for (int m = 2; m >= 0; --m) {
-                        float mat[12], vec[12];
-                        gather12(p, sm, g, m, grp, mat, vec);
+                        float mat[8], vec[8];
+                        gather8(p, sm, g, m, grp, mat, vec);
 #pragma unroll
-                        for (int i = 0; i < 12; ++i) f[i] = m == 2 ? mat[i] * vec[i] : fmaf(mat[i], vec[i], f[i]);
+                        for (int i = 0; i < 8; ++i) f[i] = m == 2 ? mat[i] * vec[i] : fmaf(mat[i], vec[i], f[i]);
 #pragma unroll
-                        for (int i = 0; i < 6; ++i) pk[m][i] = pack_bf16(mat[2 * i], mat[2 * i + 1]);
+                        for (int i = 0; i < 4; ++i) pk[m][i] = pack_bf16(mat[2 * i], mat[2 * i + 1]);
                     }
                 }
             }
-            store12(hb, t, kXCol, grp, f);
+            store_bf16x8(hb + hb_off(t, kXCol + 8 * grp), f);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                const uint32_t a4[4] = {pk[m][0], pk[m][1], pk[m][2], pk[m][3]};
-                const uint32_t a2[2] = {pk[m][4], pk[m][5]};
-                tc::st_32x32b_x4(trow(stash + 6 * m, 0), a4);
-                tc::st_32x32b_x2(trow(stash + 6 * m + 4, 0), a2);
-            }
+            for (int m = 0; m < 3; ++m) tc::st_32x32b_x4(trow(stash + 4 * m, 0), pk[m]);
             const float dIw = valid ? tab.acc[si] * w : 0.0f;
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -565,16 +514,18 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             }
             alive = wait_mma(&bar_mma, mma_phase, p.err);
             // H0 = silu(D0 + b0), this group's 32 columns
+            if (mlp) {
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                float v[16], bb[16];
-                tc::ld_32x32b_x16(trow(d0, col0 + 16 * j), v);
-                ld16(bias + col0 + 16 * j, bb);
-                tc::wait_ld();
+                for (int j = 0; j < 2; ++j) {
+                    float v[16], bb[16];
+                    tc::ld_32x32b_x16(trow(d0, col0 + 16 * j), v);
+                    ld16(bias + col0 + 16 * j, bb);
+                    tc::wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + bb[i]);
-                store_bf16x8(hb + hb_off(t, col0 + 16 * j), v);
-                store_bf16x8(hb + hb_off(t, col0 + 16 * j + 8), v + 8);
+                    for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + bb[i]);
+                    store_bf16x8(hb + hb_off(t, col0 + 16 * j), v);
+                    store_bf16x8(hb + hb_off(t, col0 + 16 * j + 8), v + 8);
+                }
             }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -587,77 +538,81 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             alive = wait_mma(&bar_mma, mma_phase, p.err) && alive;
             // last layer: partial z over this group's columns
             float a1[32];
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                float v[16], bb[16];
-                tc::ld_32x32b_x16(trow(d1, col0 + 16 * j), v);
-                ld16(bias + kH + col0 + 16 * j, bb);
-                tc::wait_ld();
-#pragma unroll
-                for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bb[i];
-            }
-            float zp = 0.f;
             __half2 gpk[16];
+            if (mlp) {
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                float ww[16];
-                ld16(bias + 2 * kH + col0 + 16 * j, ww);
+                for (int j = 0; j < 2; ++j) {
+                    float v[16], bb[16];
+                    tc::ld_32x32b_x16(trow(d1, col0 + 16 * j), v);
+                    ld16(bias + kH + col0 + 16 * j, bb);
+                    tc::wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; i += 2) {
-                    const float x0 = a1[16 * j + i], x1 = a1[16 * j + i + 1];
-                    const float s0 = sigmoid_tanh(x0), s1 = sigmoid_tanh(x1);
-                    const float h0 = x0 * s0, h1 = x1 * s1;
-                    gpk[(16 * j + i) >> 1] = __floats2half2_rn(s0 * (1.0f + x0 * (1.0f - s0)),
-                                                               s1 * (1.0f + x1 * (1.0f - s1)));
-                    a1[16 * j + i] = h0;
-                    a1[16 * j + i + 1] = h1;
-                    zp = fmaf(h0, ww[i], zp);
-                    zp = fmaf(h1, ww[i + 1], zp);
+                    for (int i = 0; i < 16; ++i) a1[16 * j + i] = v[i] + bb[i];
                 }
-            }
-            s_z[grp][t] = zp;
-            cta_barrier();
-            const float z = s_z[0][t] + s_z[1][t] + bias[3 * kH];
-            const float dz = dIw * act_grad(lact, z, beta);
-            // dA1 = dz w2 silu'(A1) into G columns col0..col0+31
+                float zp = 0.f;
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                float ww[16], da[16];
-                ld16(bias + 2 * kH + col0 + 16 * j, ww);
+                for (int j = 0; j < 2; ++j) {
+                    float ww[16];
+                    ld16(bias + 2 * kH + col0 + 16 * j, ww);
 #pragma unroll
-                for (int i = 0; i < 16; i += 2) {
-                    const float2 gg = __half22float2(gpk[(16 * j + i) >> 1]);
-                    da[i] = dz * ww[i] * gg.x;
-                    da[i + 1] = dz * ww[i + 1] * gg.y;
-                }
-                store_bf16x8(gb + g_off(t, col0 + 16 * j), da);
-                store_bf16x8(gb + g_off(t, col0 + 16 * j + 8), da + 8);
-            }
-            // last-layer weight gradient: reduce dz * silu(a1[k]) over the
-            // warp's 32 rows, halving the value set each round
-            {
-#pragma unroll
-                for (int kk = 0; kk < 32; ++kk) a1[kk] = dz * a1[kk];
-                int n = 32;
-#pragma unroll
-                for (int off = 16; off >= 1; off >>= 1) {
-                    const bool upper = (lane & off) != 0;
-                    n >>= 1;
-#pragma unroll
-                    for (int kk = 0; kk < 16; ++kk) {
-                        if (kk < n) {
-                            const float send = upper ? a1[kk] : a1[kk + n];
-                            const float keep = upper ? a1[kk + n] : a1[kk];
-                            a1[kk] = keep + __shfl_xor_sync(0xffffffffu, send, off);
-                        }
+                    for (int i = 0; i < 16; i += 2) {
+                        const float x0 = a1[16 * j + i], x1 = a1[16 * j + i + 1];
+                        const float s0 = sigmoid_tanh(x0), s1 = sigmoid_tanh(x1);
+                        const float h0 = x0 * s0, h1 = x1 * s1;
+                        gpk[(16 * j + i) >> 1] = __floats2half2_rn(s0 * (1.0f + x0 * (1.0f - s0)),
+                                                                   s1 * (1.0f + x1 * (1.0f - s1)));
+                        a1[16 * j + i] = h0;
+                        a1[16 * j + i + 1] = h1;
+                        zp = fmaf(h0, ww[i], zp);
+                        zp = fmaf(h1, ww[i + 1], zp);
                     }
                 }
-                gw2 += a1[0];
-                if (grp == 0) {
-                    float s = dz;
+                s_z[grp][t] = zp;
+            }
+            cta_barrier();
+            if (mlp) {
+                const float z = s_z[0][t] + s_z[1][t] + bias[3 * kH];
+                const float dz = dIw * act_grad(lact, z, beta);
+                // dA1 = dz w2 silu'(A1) into G columns col0..col0+31
 #pragma unroll
-                    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-                    if (lane == 0) gb2 += s;
+                for (int j = 0; j < 2; ++j) {
+                    float ww[16], da[16];
+                    ld16(bias + 2 * kH + col0 + 16 * j, ww);
+#pragma unroll
+                    for (int i = 0; i < 16; i += 2) {
+                        const float2 gg = __half22float2(gpk[(16 * j + i) >> 1]);
+                        da[i] = dz * ww[i] * gg.x;
+                        da[i + 1] = dz * ww[i + 1] * gg.y;
+                    }
+                    store_bf16x8(gb + g_off(t, col0 + 16 * j), da);
+                    store_bf16x8(gb + g_off(t, col0 + 16 * j + 8), da + 8);
+                }
+                // last-layer weight gradient: reduce dz * silu(a1[k]) over the
+                // warp's 32 rows, halving the value set each round
+                {
+#pragma unroll
+                    for (int kk = 0; kk < 32; ++kk) a1[kk] = dz * a1[kk];
+                    int n = 32;
+#pragma unroll
+                    for (int off = 16; off >= 1; off >>= 1) {
+                        const bool upper = (lane & off) != 0;
+                        n >>= 1;
+#pragma unroll
+                        for (int kk = 0; kk < 16; ++kk) {
+                            if (kk < n) {
+                                const float send = upper ? a1[kk] : a1[kk + n];
+                                const float keep = upper ? a1[kk + n] : a1[kk];
+                                a1[kk] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+                            }
+                        }
+                    }
+                    gw2 += a1[0];
+                    if (grp == 0) {
+                        float s = dz;
+#pragma unroll
+                        for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+                        if (lane == 0) gb2 += s;
+                    }
                 }
             }
             tc::fence_smem_to_async();
@@ -676,17 +631,19 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             }
             alive = wait_mma(&bar_mma, mma_phase, p.err) && alive;
             // dA0 = dH0 silu'(A0) into G columns 64 + col0.. (A0 = D0 + b0)
+            if (mlp) {
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                float gv[16], av[16], da[16], bb[16];
-                tc::ld_32x32b_x16(trow(d1, col0 + 16 * j), gv);
-                tc::ld_32x32b_x16(trow(d0, col0 + 16 * j), av);
-                ld16(bias + col0 + 16 * j, bb);
-                tc::wait_ld();
+                for (int j = 0; j < 2; ++j) {
+                    float gv[16], av[16], da[16], bb[16];
+                    tc::ld_32x32b_x16(trow(d1, col0 + 16 * j), gv);
+                    tc::ld_32x32b_x16(trow(d0, col0 + 16 * j), av);
+                    ld16(bias + col0 + 16 * j, bb);
+                    tc::wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bb[i]);
-                store_bf16x8(gb + g_off(t, kH + col0 + 16 * j), da);
-                store_bf16x8(gb + g_off(t, kH + col0 + 16 * j + 8), da + 8);
+                    for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bb[i]);
+                    store_bf16x8(gb + g_off(t, kH + col0 + 16 * j), da);
+                    store_bf16x8(gb + g_off(t, kH + col0 + 16 * j + 8), da + 8);
+                }
             }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -717,45 +674,37 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             // (HB columns 24 m + c), the tap column of the line MMA's A operand
             // (group 0), and dX * line values (the plane-gradient
             // contributions) in registers
-            float dx[12];
-            uint32_t pkr[3][6];
+            float dx[8];
+            uint32_t pkr[3][4];
             tc::wait_st();  // the feature step's TMEM stores of the plane values
-            tld12(d0, 0, grp, dx);
+            tc::ld_32x32b_x8(trow(d0, 8 * grp), dx);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                uint32_t a4[4], a2[2];
-                tc::ld_32x32b_x4(trow(stash + 6 * m, 0), a4);
-                tc::ld_32x32b_x2(trow(stash + 6 * m + 4, 0), a2);
-                tc::wait_ld();
-#pragma unroll
-                for (int i = 0; i < 4; ++i) pkr[m][i] = a4[i];
-                pkr[m][4] = a2[0];
-                pkr[m][5] = a2[1];
-            }
-            float gv[3][12];
+            for (int m = 0; m < 3; ++m) tc::ld_32x32b_x4(trow(stash + 4 * m, 0), pkr[m]);
+            tc::wait_ld();
+            float gv[3][8];
             if (real) {
                 if (grp == 0) {
                     const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
                     for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(gb + g_off(t, 8 * q)) = z4;
                 }
-                float tsum = 0.f;  // sum of |dX * line value| of this thread's 36 values
+                float tsum = 0.f;  // sum of |dX * line value| of this thread's 24 values
 #pragma unroll
                 for (int m = 0; m < 3; ++m) {
-                    float lv[12];
+                    float lv[8];
 #pragma unroll
-                    for (int i = 0; i < 12; ++i) gv[m][i] = lv[i] = 0.f;
+                    for (int i = 0; i < 8; ++i) gv[m][i] = lv[i] = 0.f;
                     if (valid) {
-                        float mat[12], vec[12];
+                        float mat[8], vec[8];
 #pragma unroll
-                        for (int i = 0; i < 6; ++i) {
+                        for (int i = 0; i < 4; ++i) {
                             const float2 x = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pkr[m][i]));
                             mat[2 * i] = x.x;
                             mat[2 * i + 1] = x.y;
                         }
-                        line12(p, g, m, grp, vec);
+                        line8(p, g, m, grp, vec);
 #pragma unroll
-                        for (int i = 0; i < 12; ++i) {
+                        for (int i = 0; i < 8; ++i) {
                             gv[m][i] = dx[i] * vec[i];
                             tsum += fabsf(gv[m][i]);
                             lv[i] = dx[i] * mat[i];
@@ -777,14 +726,14 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                             }
                         } else {  // outside the item's window: straight to global
 #pragma unroll
-                            for (int i = 0; i < 12; ++i) {
-                                const int c = chan12(grp, i);
+                            for (int i = 0; i < 8; ++i) {
+                                const int c = 8 * grp + i;
                                 atomicAdd(&p.gfield.line[m][l.x0 * kC + c], l.w0 * lv[i]);
                                 atomicAdd(&p.gfield.line[m][l.x1 * kC + c], l.w1 * lv[i]);
                             }
                         }
                     }
-                    store12(hb, t, kC * m, grp, lv);
+                    store_bf16x8(hb + hb_off(t, kC * m + 8 * grp), lv);
                 }
                 // The bilinear weights of a sample sum to 1, so the tile adds at
                 // most sum |dX * line value| to any texel of the slot.
@@ -828,29 +777,27 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     }
                     tc::commit(&bar_mma);
                 }
-                // scatter, phase 2: the group's 12 channels to the four
+                // scatter, phase 2: the group's 8 channels to the four
                 // corners, as fixed-point integers (shared-memory integer
                 // atomics run several times faster than FP32 ones); the lane's
-                // channel order is rotated so a warp's atomics spread over banks
+                // corner order is rotated so a warp's atomics spread over
+                // texels. Channels go in a fixed order, which keeps the 24
+                // contributions in registers.
                 if (valid) {
-                    const int rot = lane % 12;
-#pragma unroll 1
+#pragma unroll
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
                         const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
                         if (to_smem) {
-                            int* GP = gpl + p.gplane_off[m];
+                            int* GP = gpl + gpo[m];
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
                                 float wj;
-                                const int tx = corner_texel(kc, j, Wm, wj) * kC;
+                                const int tx = corner_texel(kc, (j + lane) & 3, Wm, wj) * kGP;
                                 const float ws = wj * scale;
 #pragma unroll
-                                for (int r = 0; r < 12; ++r) {
-                                    int i = r + rot;
-                                    i = i >= 12 ? i - 12 : i;
-                                    atomicAdd(&GP[tx + chan12(grp, i)], __float2int_rn(ws * gv[m][i]));
-                                }
+                                for (int i = 0; i < 8; ++i)
+                                    atomicAdd(&GP[tx + 8 * grp + i], __float2int_rn(ws * gv[m][i]));
                             }
                         } else {
                             float* GG = p.gfield.plane[m] + it.slot * (int64_t)(Hm * Wm * kC);
@@ -859,23 +806,24 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                                 float wj;
                                 const int tx = corner_texel(kc, j, Wm, wj) * kC;
 #pragma unroll
-                                for (int i = 0; i < 12; ++i) atomicAdd(&GG[tx + chan12(grp, i)], wj * gv[m][i]);
+                                for (int i = 0; i < 8; ++i) atomicAdd(&GG[tx + 8 * grp + i], wj * gv[m][i]);
                             }
                         }
                     }
                 }
                 alive = wait_mma(&bar_mma, mma_phase, p.err) && alive;
-                float v0[12], v1[12], v2[12];
-                tld12(d0, 0, grp, v0);
-                tld12(d0, kC, grp, v1);
-                tld12(d0, 2 * kC, grp, v2);
+                float v0[8], v1[8], v2[8];
+                tc::ld_32x32b_x8(trow(d0, 8 * grp), v0);
+                tc::ld_32x32b_x8(trow(d0, kC + 8 * grp), v1);
+                tc::ld_32x32b_x8(trow(d0, 2 * kC + 8 * grp), v2);
+                tc::wait_ld();
                 if (t < 3 * kLineRows) {
                     const int m = t / kLineRows, i = t % kLineRows;
-                    float* dst = gln + (m * kLineWin + i) * kC;
+                    float* dst = gln + (m * kLineWin + i) * kC + 8 * grp;
 #pragma unroll
-                    for (int q = 0; q < 12; ++q) {
+                    for (int q = 0; q < 8; ++q) {
                         const float v = m == 0 ? v0[q] : (m == 1 ? v1[q] : v2[q]);
-                        if (v != 0.0f) atomicAdd(dst + chan12(grp, q), v);
+                        if (v != 0.0f) atomicAdd(dst + q, v);
                     }
                 }
             }
@@ -891,9 +839,11 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             for (int m = 0; m < 3; ++m) {
                 const int pf = p.field.plane_h[m] * p.field.plane_w[m] * kC;
                 float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
-                const int* src = gpl + p.gplane_off[m];
+                const int* src = gpl + gpo[m];
                 for (int i = tid * 4; i < pf; i += kThreadsB * 4) {
-                    const int4 q = *reinterpret_cast<const int4*>(src + i);
+                    // 4 channels of one texel (24 is a multiple of 4)
+                    const int* e = src + (i / kC) * kGP + i % kC;
+                    const int4 q = make_int4(e[0], e[1], e[2], e[3]);
                     const float4 v =
                         make_float4((float)q.x * inv, (float)q.y * inv, (float)q.z * inv, (float)q.w * inv);
                     if (fb)
@@ -912,14 +862,14 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
         }
         __syncthreads();
     }
-    // decoder gradients from the TMEM accumulator rows (group 0 reads columns
-    // 0..47, group 1 columns 48..95): rows 0..63 hold dW1 (columns 0..63) and
-    // db1 (column 88), rows 64..127 dW0 (columns 64..87) and db0 (column 88)
+    // decoder gradients from the TMEM accumulator rows (group g reads columns
+    // 32g .. 32g + 31): rows 0..63 hold dW1 (columns 0..63) and db1 (column
+    // 88), rows 64..127 dW0 (columns 64..87) and db0 (column 88)
     if (had_tile) {
         tc::fence_after_sync();
 #pragma unroll
-        for (int jj = 0; jj < 3; ++jj) {
-            const int j = 3 * grp + jj;
+        for (int jj = 0; jj < 2; ++jj) {
+            const int j = 2 * grp + jj;
             float v[16];
             tc::ld_32x32b_x16(trow(dacc, 16 * j), v);
             tc::wait_ld();
@@ -942,7 +892,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
         }
     }
     // last layer: lane l's column within its group's 32, by the halving order
-    {
+    if (mlp) {
         int colbits = 0;
         for (int off = 16, b = 0; off >= 1; off >>= 1, ++b)
             if (lane & off) colbits |= (32 >> (b + 1));
@@ -978,9 +928,12 @@ static int launch24(void (*fn)(FusedParams), bool bwd, const FusedParams& p, cud
     const int threads = bwd ? tc24::kThreadsB : tc24::kThreadsF;
     ATDF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)fn, threads, smem));
     if (per < 1) return ATDF_ERR_UNSUPPORTED;
-    // one CTA per SM: the shared memory of either kernel leaves room for one,
-    // and the backward holds all 512 TMEM columns
-    fn<<<sms, threads, smem, st>>>(p);
+    // the forward fits two CTAs per SM (shared memory, 2 x 256 TMEM columns);
+    // the backward one (its shared memory, all 512 TMEM columns)
+    int smem_sm = 0;
+    ATDF_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    per = bwd ? 1 : std::max(1, std::min(2, smem_sm / (smem + 1024)));
+    fn<<<sms * per, threads, smem, st>>>(p);
     ATDF_LAUNCH_CHECK();
     return ATDF_OK;
 }

@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--no-psnr30", action="store_true", help="skip the seconds-to-30 dB runs")
     ap.add_argument("--psnr-target", type=float, default=18.0)
     ap.add_argument("--psnr-epochs", type=int, default=3)
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="only run this many forward + backward projections of the workload's BF16 form (no "
+                         "timing, no JSON line): the program a profiler captures")
+    ap.add_argument("--workload", default="C5", help="configuration of --profile-steps (C2 or C5)")
     return ap.parse_args()
 
 
@@ -820,8 +824,37 @@ def make_host_shapes(R):
     return [torch.empty(R, 3), torch.empty(R, 3), torch.empty(1, R)]
 
 
+def run_profile(args):
+    """--profile-steps: the BF16 form's fused forward and backward on one
+    batch of the workload, repeated, for ncu."""
+    import torch
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+
+    cfg = dataclasses.replace(workload_config(args.workload), rays_per_batch=args.rays)
+    tree, dev, _, nseg, nsamp = prepare_workload(cfg, args.rays, 0, nb=1)
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    o, d, _ = dev[0]
+    rays = ab.RayList(o, d)
+    for k in range(args.profile_steps):
+        img = geo.ProjectRays(tree, rays, cfg.max_samples_per_node, 1 + k)
+        img.sum().backward()
+        for prm in syn.parameters(geo):
+            prm.grad = None
+    torch.cuda.synchronize()
+    geo.CheckErrors()
+    print(json.dumps({"profile_steps": args.profile_steps, "workload": cfg.name, "rays": args.rays,
+                      "segments": nseg, "samples": nsamp}), flush=True)
+
+
 def main():
     args = parse()
+    if args.profile_steps:
+        run_profile(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1 and args.impl == "ours":

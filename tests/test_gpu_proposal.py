@@ -264,7 +264,17 @@ def test_proposal_kernels_match_restatement(oracle):
         w = xw.cpu().numpy()
         ln = np.repeat(b["tmax"] - b["tmin"], b["n"])
         assert np.abs(t - t_ref).max() <= 1e-4 * max(1.0, ln.max())
-        assert rel_err(w, w_ref) < 1e-4
+        if rule == 0:
+            assert rel_err(w, w_ref) < 1e-4
+        else:
+            # importance weights jump at bin edges: a sample within rounding
+            # of an edge may fall in either bin (FP32 CDF on the GPU, FP64
+            # in the restatement); every other weight agrees
+            t0r = np.repeat(b["tmin"], b["n"])
+            pos = (t_ref - t0r) / np.maximum(ln, 1e-30) * po.BINS
+            near_edge = np.abs(pos - np.round(pos)) < 1e-3
+            ok = np.abs(w - w_ref) <= 1e-4 * np.abs(w_ref)
+            assert np.all(ok | near_edge) and ok.mean() > 0.999
         seg = np.repeat(np.arange(G), b["n"])
         assert np.all(t >= b["tmin"][seg]) and np.all(t <= b["tmax"][seg])
     # loss, its gradient, and the occupancy sums
