@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-psnr", action="store_true", help="skip the seconds-to-PSNR runs")
     ap.add_argument("--no-psnr30", action="store_true", help="skip the seconds-to-30 dB runs")
+    ap.add_argument("--no-gate", action="store_true", help="skip the proposal's 400-step gate run on C5")
     ap.add_argument("--psnr-target", type=float, default=18.0)
     ap.add_argument("--psnr-epochs", type=int, default=3)
     ap.add_argument("--profile-steps", type=int, default=0,
@@ -310,6 +311,44 @@ def measure_proposal(args, tree, cfg, dev_batches, nb, stream, budget):
                 "rays_per_s_proposal_steps": R / (res["proposal_step_ms"] * 1e-3),
                 "rays_per_s_with_judge_every_10": R / (amort * 1e-3)})
     del geo, opt, params, ps
+    return res
+
+
+def proposal_gate(tree, cfg, dev_batches, budget, steps=400):
+    """Does the proposal hold the 1% gate at this budget? Trains the BF16
+    form from the seeded initialisation through the proposal schedule (judge
+    every 10th step, every step in the 20-step warm-up) for `steps` steps on
+    the workload's batches and reports the schedule's counters, the last
+    judge's projection error and the error every 100 steps."""
+    import torch
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+    from adaptivetensordf_b200.optim import Adam
+    from adaptivetensordf_b200.proposal import ProposalSchedule
+
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003, init_scale=0.05)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    opt = Adam([{"params": list(geo.planes) + list(geo.lines), "lr": 0.01},
+                {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": 5e-4}], geometry=geo)
+    prop = ProposalSchedule(tree, geo, cfg.max_samples_per_node, budget=budget)
+    trace = []
+    t0 = time.perf_counter()
+    for k in range(steps):
+        o, d, y = dev_batches[k % len(dev_batches)]
+        img = prop.project(ab.RayList(o, d), 1 + k, y)
+        loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
+        img.backward(gimg)
+        opt.step()
+        opt.zero_grad(set_to_none=True)
+        if k % 100 == 99:
+            trace.append([k + 1, prop.last_error])
+    torch.cuda.synchronize()
+    geo.CheckErrors()
+    res = {"budget_per_ray": budget, "steps": steps, "gate": prop.gate, "error_trace": trace,
+           "wall_s": time.perf_counter() - t0, **prop.stats()}
+    del geo, opt, prop
     return res
 
 
@@ -645,6 +684,8 @@ def run_ours(args, rank, world):
     sampler = ClockSampler(local)
     r5 = measure_form(args, tree, cfg, "bf16", dev, host, world, sampler)
     prop5 = measure_proposal(args, tree, cfg, dev, len(dev), stream, 64) if world == 1 else None
+    if prop5 is not None and not args.no_gate:
+        prop5["gate_run"] = proposal_gate(tree, cfg, dev, 64)
     del tree, dev, host
 
     # the depth-4 / rank-16 workload: plain FP32 against the chosen form

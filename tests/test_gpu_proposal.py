@@ -551,3 +551,68 @@ def test_proposal_mlp_tensor_core_kernels_with_no_segments():
     torch.cuda.synchronize()
     assert torch.all(out == 7.0) and int(err.item()) == 0
     assert all(float(t.abs().sum()) == 0.0 for t in gw + gb)
+
+
+def test_c5_proposal_holds_gate_at_64_samples_per_ray():
+    """On the C5 slab (depth-6 adaptive tree, rank 24, 256 uniform samples per
+    ray on average) the proposal trained online through the schedule serves
+    the training steps at 64 samples per ray, a quarter of the uniform
+    count: after 300 steps its projection error against the uniform judge is
+    inside the 1% gate, and a step through its samples costs at most 0.7 of a
+    uniform step."""
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+    from adaptivetensordf_b200.optim import Adam
+    from adaptivetensordf_b200.proposal import ProposalSchedule
+
+    cfg = syn.CONFIGS["C5"]
+    ph = syn.config_phantom(cfg, 1001)
+    tree = syn.adaptive_tree(cfg, ph, device="cuda")
+    batches = []
+    for b in range(6):
+        o, d = syn.random_ray_batch(cfg, cfg.rays_per_batch, 5000 + b)
+        y = syn.analytic_projection(ph, o, d, device="cuda").astype(np.float32)
+        batches.append((torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda(), torch.from_numpy(y).cuda()))
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003, init_scale=0.05)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    opt = Adam([{"params": list(geo.planes) + list(geo.lines), "lr": 0.01},
+                {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": 5e-4}], geometry=geo)
+    prop = ProposalSchedule(tree, geo, cfg.max_samples_per_node, budget=64)
+
+    def step(k, mode):
+        o, d, y = batches[k % len(batches)]
+        rays = ab.RayList(o, d)
+        if mode == "schedule":
+            img = prop.project(rays, 1 + k, y)
+        elif mode == "proposal":
+            img = prop.ps.Project(tree, geo, rays, 1 + k)
+        else:
+            img = geo.ProjectRays(tree, rays, cfg.max_samples_per_node, 1 + k)
+        loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
+        img.backward(gimg)
+        opt.step()
+        opt.zero_grad(set_to_none=True)
+
+    for k in range(300):
+        step(k, "schedule")
+    st = prop.stats()
+    ms = {}
+    for mode in ("proposal", "uniform"):
+        step(0, mode)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(10):
+            step(400 + k, mode)
+        e1.record()
+        torch.cuda.synchronize()
+        ms[mode] = e0.elapsed_time(e1) / 10
+    geo.CheckErrors()
+    nuni = tree.CreateSamplesForRays(ab.RayList(*batches[0][:2]), cfg.max_samples_per_node, False).size()
+    print(f"\nC5 proposal at 64 samples/ray (uniform {nuni / cfg.rays_per_batch:.0f}): error {st['proposal_error']:.4f}, "
+          f"{st['proposal_steps']} proposal / {st['judge_steps']} judge / {st['uniform_steps']} uniform steps; "
+          f"step {ms['proposal']:.2f} ms vs uniform {ms['uniform']:.2f} ms")
+    assert nuni / cfg.rays_per_batch > 200
+    assert st["proposal_open"] and st["proposal_error"] <= 0.01
+    assert st["proposal_steps"] > 200
+    assert ms["proposal"] < 0.7 * ms["uniform"]
