@@ -51,8 +51,13 @@ constexpr int kHBCols = 96;      // H0 (64) | X (24) | ones | zero pad
 constexpr int kXCol = 64;
 constexpr int kOnesCol = 88;
 constexpr int kGCols = 128;      // dA1 (64) | dA0 (64)
-constexpr int kLineWin = 32;     // line-gradient window entries per line (shared memory)
-constexpr int kLineRows = 21;    // rows per line in the line-gradient MMA (3 lines <= 64 rows)
+// The backward keeps a window of kLineRows rows of each line per slot: the
+// rows of the line values it reads (staged in shared memory) and of the line
+// gradients it accumulates (in TMEM, by the line MMA). A leaf of depth d spans
+// 256 / 2^d cells of a 256-entry line, so 42 rows cover depth-3 leaves (32
+// cells, both taps and a rounding margin); samples outside the window read
+// and add to global memory.
+constexpr int kLineRows = 42;    // 3 x 42 = 126 <= 128 rows of the line MMA
 constexpr int kLineN = 80;       // N of the line-gradient MMA (3 * 24 = 72, padded)
 constexpr int kThreadsF = 256;   // forward: two halves of 128 rows, one thread per row
 constexpr int kThreadsB = 384;   // backward: one half of 128 rows, three threads per row
@@ -71,7 +76,7 @@ __device__ __forceinline__ uint32_t w0_off(int n, int f) { return tc::kmajor_off
 __device__ __forceinline__ uint32_t w1_off(int n, int k) { return tc::kmajor_off(n, k, kH); }
 
 struct Smem24 {
-    uint32_t planes, w0, w1, bias, hb[2], g, gplanes, gline, segi, total;
+    uint32_t planes, w0, w1, bias, hb[2], g, gplanes, lwin, segi, total;
     // gplane_elems: the unpadded plane-gradient elements (texels x 24)
     __host__ __device__ Smem24(int plane_elems, int gplane_elems, bool bwd)
     {
@@ -93,8 +98,8 @@ struct Smem24 {
         if (bwd) o = al(o + kRows * kGCols * 2);
         gplanes = o;
         if (bwd) o = al(o + ((gplane_elems / kC * kGP + 3) & ~3) * 4);
-        gline = o;
-        if (bwd) o = al(o + 3 * kLineWin * kC * 4);
+        lwin = o;  // BF16 rows of the slot's line windows
+        if (bwd) o = al(o + 3 * kLineRows * kC * 2);
         segi = o;
         // the forward's table keeps a sample -> segment map of kMapCapF
         // samples only, which lets two forward CTAs share an SM
@@ -331,10 +336,25 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cta_barrier() { asm volatile("bar.sync 1, 384;" ::: "memory"); }
 
+// First row of line m's window for the slot whose leaf box (min, size) is
+// `box`: two rows below the leaf's first cell, clamped to the line.
+__device__ __forceinline__ int line_window_lo(const FusedParams& p, const float* box, int m)
+{
+    const int Ln = p.field.line_len[m];
+    if (Ln <= kLineRows) return 0;
+    // x line: the ROI-normalised x; z line: the raw z; y line: the local y
+    const float u = m == 0 ? roi_coord(box[0], p.field.roi_min[0], p.field.roi_max[0]) : (m == 2 ? box[2] : -1.0f);
+    const int lo = (int)floorf(((u + 1.0f) * 0.5f) * (float)(Ln - 1)) - 2;
+    return max(0, min(lo, Ln - kLineRows));
+}
+
 // Plane (bilinear) and line (linear) values of plane / line m for the 8
-// channels of group g (channels 8g .. 8g + 7) of one sample.
-__device__ __forceinline__ void gather8(const FusedParams& p, const unsigned char* sm, const SampleGeo& g, int m,
-                                        int grp, float (&mat)[8], float (&vec)[8])
+// channels of group g (channels 8g .. 8g + 7) of one sample. The line rows
+// come from the slot's window in shared memory (LW: kLineRows rows of 24
+// BF16 channels from row lo) when both taps are inside it.
+__device__ __forceinline__ void gather8(const FusedParams& p, const unsigned char* sm, const unsigned char* LW,
+                                        int lo, const SampleGeo& g, int m, int grp, float (&mat)[8],
+                                        float (&vec)[8])
 {
     const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m], L = p.field.line_len[m];
     const int Wp = p.plane_pitch[m];
@@ -348,21 +368,20 @@ __device__ __forceinline__ void gather8(const FusedParams& p, const unsigned cha
 #pragma unroll
         for (int i = 0; i < 8; ++i) mat[i] = j == 0 ? u[i] * w : fmaf(u[i], w, mat[i]);
     }
-    const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]) + 16 * grp;
+    const int r0 = l.x0 - lo, r1 = l.x1 - lo;
+    uint4 q0, q1;
+    if ((unsigned)r0 < (unsigned)kLineRows && (unsigned)r1 < (unsigned)kLineRows) {
+        const unsigned char* V = LW + (size_t)m * (kLineRows * kC * 2) + 16 * grp;
+        q0 = *reinterpret_cast<const uint4*>(V + r0 * (kC * 2));
+        q1 = *reinterpret_cast<const uint4*>(V + r1 * (kC * 2));
+    } else {
+        const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]) + 16 * grp;
+        q0 = __ldg(reinterpret_cast<const uint4*>(V + l.x0 * (kC * 2)));
+        q1 = __ldg(reinterpret_cast<const uint4*>(V + l.x1 * (kC * 2)));
+    }
     float v0[8], v1[8];
-    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x0 * (kC * 2))), v0);
-    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x1 * (kC * 2))), v1);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
-}
-
-__device__ __forceinline__ void line8(const FusedParams& p, const SampleGeo& g, int m, int grp, float (&vec)[8])
-{
-    const Corner1 l = corners1(g.lu[m], p.field.line_len[m]);
-    const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]) + 16 * grp;
-    float v0[8], v1[8];
-    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x0 * (kC * 2))), v0);
-    unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x1 * (kC * 2))), v1);
+    unpack_bf16x8(q0, v0);
+    unpack_bf16x8(q1, v1);
 #pragma unroll
     for (int i = 0; i < 8; ++i) vec[i] = fmaf(v0[i], l.w0, v1[i] * l.w1);
 }
@@ -399,11 +418,13 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = s_tmem;
-    // TMEM: D0 / dX (0..63), D1 / dH0 (64..127), the line MMA over 0..79 once
-    // both are consumed, the weight-gradient accumulator (128..223), and the
-    // BF16 plane values of the feature step (256 + 12 g .. 256 + 12 g + 11)
-    const uint32_t d0 = tbase, d1 = tbase + 64, dacc = tbase + 128;
-    const uint32_t stash = tbase + 256 + 12 * grp;
+    // TMEM: D0 / dX (0..63), D1 / dH0 (64..127), the weight-gradient
+    // accumulator (128..223), the BF16 plane values of the feature step
+    // (256 + 12 g .. + 11), the slot's line-gradient accumulator (320..399;
+    // row m * kLineRows + i, columns 24 m + c) and the FP32 line values of the
+    // feature step (400 + 24 g .. + 23)
+    const uint32_t d0 = tbase, d1 = tbase + 64, dacc = tbase + 128, dline = tbase + 320;
+    const uint32_t stash = tbase + 256 + 12 * grp, vstash = tbase + 400 + 24 * grp;
     SegTab tab = seg_tab(reinterpret_cast<float*>(sm + L.segi));
     const float* bias = reinterpret_cast<const float*>(sm + L.bias);
     const float beta = p.mlp.softplus_beta;
@@ -413,7 +434,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     const int gpl_words = (p.gplane_off[3] / kC * kGP + 3) & ~3;
     const int gpo[3] = {p.gplane_off[0] / kC * kGP, p.gplane_off[1] / kC * kGP, p.gplane_off[2] / kC * kGP};
     int* gpl = reinterpret_cast<int*>(sm + L.gplanes);
-    float* gln = reinterpret_cast<float*>(sm + L.gline);
+    unsigned char* lw = sm + L.lwin;
     unsigned char* hb = sm + L.hb[0];
     unsigned char* gb = sm + L.g;
     uint32_t tma_phase = 0, mma_phase = 0;
@@ -421,6 +442,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group (groups 0, 1)
     float scale = 0.f;           // the slot's fixed-point scale
     int ntiles = 0;              // tiles of the slot
+    bool lacc = false;           // the line MMA has written the slot's accumulator
     while (alive) {
         const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
         if (it.slot < 0) break;
@@ -444,18 +466,18 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             }
             scale = 0.f;
             ntiles = 0;
-            for (int i = tid; i < 3 * kLineWin * kC; i += kThreadsB) gln[i] = 0.0f;
-            if (tid < 3) {
-                const float* bmin = tab.box;  // the item's leaf (segment 0's)
-                const int Ln = p.field.line_len[tid];
-                int lo = 0;
-                if (Ln > kLineRows) {
-                    const float u = tid == 0 ? roi_coord(bmin[0], p.field.roi_min[0], p.field.roi_max[0])
-                                             : (tid == 2 ? bmin[2] : -1.0f);
-                    lo = (int)floorf(((u + 1.0f) * 0.5f) * (float)(Ln - 1)) - 2;
-                    lo = max(0, min(lo, Ln - kLineRows));
-                }
-                s_lo[tid] = lo;
+            lacc = false;
+            // the slot's line windows (the item's leaf is segment 0's): rows
+            // lo .. lo + kLineRows - 1 of each line, 3 x 16 bytes per row
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const int lo = line_window_lo(p, tab.box, m);
+                if (tid == 0) s_lo[m] = lo;
+                const int n16 = 3 * min(kLineRows, p.field.line_len[m] - lo);
+                const uint4* src = reinterpret_cast<const uint4*>(
+                    reinterpret_cast<const unsigned char*>(p.field.line[m]) + (size_t)lo * (kC * 2));
+                uint4* dst = reinterpret_cast<uint4*>(lw + m * (kLineRows * kC * 2));
+                for (int i = tid; i < n16; i += kThreadsB) dst[i] = __ldg(src + i);
             }
             if (!mbar_wait(&bar_tma, tma_phase)) {
                 set_err(p.err, ATDF_DEVERR_TREE);
@@ -471,38 +493,39 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             const bool handshake = !scale_set && t0 == 0;
             const int k = t0 + t;
             const bool valid = k < it.total;
-            // features (own 8 channels), plane values kept as BF16 in TMEM
+            // features (own 8 channels); the plane values (BF16) and the line
+            // values (FP32) go to TMEM for the scatter
             SampleGeo g;
             float w = 0.0f;
             int si = -1;
-            float f[8];
-            uint32_t pk[3][4];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) f[i] = 0.0f;
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-#pragma unroll
-                for (int i = 0; i < 4; ++i) pk[m][i] = 0u;
+            bool act = false;
             if (valid) {
                 const SampleState st = sample_state(p, tab, it, k);
                 w = st.w;
                 si = st.si;
                 if (real) {
                     g = sample_geo_fast(p, tab, st.node, st.pos);
-#pragma unroll
-                    for (int m = 2; m >= 0; --m) {
-                        float mat[8], vec[8];
-                        gather8(p, sm, g, m, grp, mat, vec);
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) f[i] = m == 2 ? mat[i] * vec[i] : fmaf(mat[i], vec[i], f[i]);
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) pk[m][i] = pack_bf16(mat[2 * i], mat[2 * i + 1]);
-                    }
+                    act = true;
                 }
             }
-            store_bf16x8(hb + hb_off(t, kXCol + 8 * grp), f);
+            float f[8];
 #pragma unroll
-            for (int m = 0; m < 3; ++m) tc::st_32x32b_x4(trow(stash + 4 * m, 0), pk[m]);
+            for (int m = 2; m >= 0; --m) {
+                float mat[8], vec[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) mat[i] = vec[i] = 0.0f;
+                if (act) gather8(p, sm, lw, s_lo[m], g, m, grp, mat, vec);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) f[i] = m == 2 ? mat[i] * vec[i] : fmaf(mat[i], vec[i], f[i]);
+                uint32_t pk[4], vb[8];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) pk[i] = pack_bf16(mat[2 * i], mat[2 * i + 1]);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) vb[i] = __float_as_uint(vec[i]);
+                tc::st_32x32b_x4(trow(stash + 4 * m, 0), pk);
+                tc::st_32x32b_x8(trow(vstash + 8 * m, 0), vb);
+            }
+            store_bf16x8(hb + hb_off(t, kXCol + 8 * grp), f);
             const float dIw = valid ? tab.acc[si] * w : 0.0f;
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -676,7 +699,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             // contributions) in registers
             float dx[8];
             uint32_t pkr[3][4];
-            tc::wait_st();  // the feature step's TMEM stores of the plane values
+            tc::wait_st();  // the feature step's TMEM stores of the plane and line values
             tc::ld_32x32b_x8(trow(d0, 8 * grp), dx);
 #pragma unroll
             for (int m = 0; m < 3; ++m) tc::ld_32x32b_x4(trow(stash + 4 * m, 0), pkr[m]);
@@ -686,23 +709,24 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                 if (grp == 0) {
                     const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(gb + g_off(t, 8 * q)) = z4;
+                    for (int q = 0; q < kGCols / 8; ++q) *reinterpret_cast<uint4*>(gb + g_off(t, 8 * q)) = z4;
                 }
                 float tsum = 0.f;  // sum of |dX * line value| of this thread's 24 values
 #pragma unroll
                 for (int m = 0; m < 3; ++m) {
-                    float lv[8];
+                    float lv[8], vec[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) gv[m][i] = lv[i] = 0.f;
+                    tc::ld_32x32b_x8(trow(vstash + 8 * m, 0), vec);
+                    tc::wait_ld();
                     if (valid) {
-                        float mat[8], vec[8];
+                        float mat[8];
 #pragma unroll
                         for (int i = 0; i < 4; ++i) {
                             const float2 x = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&pkr[m][i]));
                             mat[2 * i] = x.x;
                             mat[2 * i + 1] = x.y;
                         }
-                        line8(p, g, m, grp, vec);
 #pragma unroll
                         for (int i = 0; i < 8; ++i) {
                             gv[m][i] = dx[i] * vec[i];
@@ -724,7 +748,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                                         __float2bfloat16_rn(l.w1);
                                 }
                             }
-                        } else {  // outside the item's window: straight to global
+                        } else {  // outside the slot's window: straight to global
 #pragma unroll
                             for (int i = 0; i < 8; ++i) {
                                 const int c = 8 * grp + i;
@@ -764,7 +788,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                 const bool to_smem =
                     s_tcum * scale + (float)ntiles * (0.5f * kRows * 3 * 4 * kC) <= 1073741824.0f;
                 if (!to_smem && issuer) s_fb = 1;
-                if (issuer) {  // line gradients of the tile (overlaps the plane atomics)
+                if (issuer) {  // line gradients of the tile into the slot's accumulator (overlaps the atomics)
                     tc::fence_after_sync();
                     const uint32_t abase = tc::smem_addr(gb), bbase = tc::smem_addr(hb);
 #pragma unroll
@@ -773,10 +797,11 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                             tc::smem_desc(abase + j * 2 * (kGCols / 8) * 128, (kGCols / 8) * 128, 128);
                         const uint64_t b =
                             tc::smem_desc(bbase + j * 2 * (kHBCols / 8) * 128, (kHBCols / 8) * 128, 128);
-                        tc::mma_bf16(d0, a, b, tc::idesc_bf16(kRows, kLineN, 1, 1), j > 0 ? 1u : 0u);
+                        tc::mma_bf16(dline, a, b, tc::idesc_bf16(kRows, kLineN, 1, 1), (lacc || j > 0) ? 1u : 0u);
                     }
                     tc::commit(&bar_mma);
                 }
+                lacc = true;
                 // scatter, phase 2: the group's 8 channels to the four
                 // corners, as fixed-point integers (shared-memory integer
                 // atomics run several times faster than FP32 ones); the lane's
@@ -812,20 +837,6 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     }
                 }
                 alive = wait_mma(&bar_mma, mma_phase, p.err) && alive;
-                float v0[8], v1[8], v2[8];
-                tc::ld_32x32b_x8(trow(d0, 8 * grp), v0);
-                tc::ld_32x32b_x8(trow(d0, kC + 8 * grp), v1);
-                tc::ld_32x32b_x8(trow(d0, 2 * kC + 8 * grp), v2);
-                tc::wait_ld();
-                if (t < 3 * kLineRows) {
-                    const int m = t / kLineRows, i = t % kLineRows;
-                    float* dst = gln + (m * kLineWin + i) * kC + 8 * grp;
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const float v = m == 0 ? v0[q] : (m == 1 ? v1[q] : v2[q]);
-                        if (v != 0.0f) atomicAdd(dst + q, v);
-                    }
-                }
             }
             tc::fence_before_sync();
             cta_barrier();
@@ -851,12 +862,28 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     else
                         *reinterpret_cast<float4*>(dst + i) = v;
                 }
-                const int Ln = p.field.line_len[m];
-                const int lo = s_lo[m];
-                for (int i = tid; i < kLineWin * kC; i += kThreadsB) {
-                    const int e = lo + i / kC;
-                    const float v = gln[m * kLineWin * kC + i];
-                    if (e < Ln && v != 0.0f) atomicAdd(&p.gfield.line[m][e * kC + (i % kC)], v);
+            }
+            // the slot's line gradients: TMEM row m * kLineRows + i holds row
+            // s_lo[m] + i of line m in columns 24 m .. 24 m + 23
+            if (lacc) {
+                tc::fence_after_sync();
+                float v0[8], v1[8], v2[8];
+                tc::ld_32x32b_x8(trow(dline, 8 * grp), v0);
+                tc::ld_32x32b_x8(trow(dline, kC + 8 * grp), v1);
+                tc::ld_32x32b_x8(trow(dline, 2 * kC + 8 * grp), v2);
+                tc::wait_ld();
+                tc::fence_before_sync();
+                if (t < 3 * kLineRows) {
+                    const int m = t / kLineRows, i = t % kLineRows;
+                    const int e = s_lo[m] + i;
+                    if (e < p.field.line_len[m]) {
+                        float* dst = p.gfield.line[m] + e * kC + 8 * grp;
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const float v = m == 0 ? v0[q] : (m == 1 ? v1[q] : v2[q]);
+                            if (v != 0.0f) atomicAdd(dst + q, v);
+                        }
+                    }
                 }
             }
         }
