@@ -468,11 +468,14 @@ __device__ __forceinline__ float sample_t_step(float tmin, float step, int j, fl
     return __fadd_rn(__fmul_rn(t1, oma), __fmul_rn(t2, a));
 }
 
+// permute: visit the item's samples in the permuted order (kernels that
+// scatter with shared-memory atomics); without it sample k is the item's k-th
+// (consecutive rows walk along a ray, so their gathers share texels).
 __device__ __forceinline__ SampleState sample_state(const FusedParams& p, const SegTab& tab, const ItemInfo& it,
-                                                    int k)
+                                                    int k, bool permute = true)
 {
     SampleState s;
-    const int kk = it.total < kSamplePermPrime ? perm_index(k, it.total, it.inv_total) : k;
+    const int kk = permute && it.total < kSamplePermPrime ? perm_index(k, it.total, it.inv_total) : k;
     s.si = it.use_map ? (int)tab.map[kk] : find_seg(tab, it.nseg, kk);
     const int j = kk - tab.start[s.si];
     const int n = tab.n[s.si];

@@ -47,7 +47,8 @@ constexpr int kC = 24;
 constexpr int kCP = 32;          // channels padded to a multiple of 16 (K of layer 0, N of dX)
 constexpr int kH = 64;
 constexpr int kRows = 128;       // samples per tile
-constexpr int kHBCols = 96;      // H0 (64) | X (24) | ones | zero pad
+constexpr int kHBCols = 96;      // backward feature buffer: H0 (64) | X (24) | ones | zero pad
+constexpr int kHBColsF = 64;     // forward: X in columns 0..31 (24..31 zero), then H0 over it
 constexpr int kXCol = 64;
 constexpr int kOnesCol = 88;
 constexpr int kGCols = 128;      // dA1 (64) | dA0 (64)
@@ -71,6 +72,7 @@ constexpr uint32_t kTmemF = 256;  // columns per forward CTA (two CTAs per SM)
 constexpr uint32_t kTmemB = 512;  // columns per backward CTA (one CTA per SM)
 
 __device__ __forceinline__ uint32_t hb_off(int s, int c) { return tc::mnmajor_off(c, s, kHBCols); }
+__device__ __forceinline__ uint32_t hbf_off(int s, int c) { return tc::mnmajor_off(c, s, kHBColsF); }
 __device__ __forceinline__ uint32_t g_off(int s, int c) { return tc::mnmajor_off(c, s, kGCols); }
 __device__ __forceinline__ uint32_t w0_off(int n, int f) { return tc::kmajor_off(n, f, kCP); }
 __device__ __forceinline__ uint32_t w1_off(int n, int k) { return tc::kmajor_off(n, k, kH); }
@@ -91,15 +93,15 @@ struct Smem24 {
         bias = o;  // b0[64] b1[64] w2[64] b2
         o = al(o + (3 * kH + 4) * 4);
         hb[0] = o;
-        o = al(o + kRows * kHBCols * 2);
+        o = al(o + kRows * (bwd ? kHBCols : kHBColsF) * 2);
         hb[1] = o;
-        if (!bwd) o = al(o + kRows * kHBCols * 2);
+        if (!bwd) o = al(o + kRows * kHBColsF * 2);
         g = o;
         if (bwd) o = al(o + kRows * kGCols * 2);
         gplanes = o;
         if (bwd) o = al(o + ((gplane_elems / kC * kGP + 3) & ~3) * 4);
         lwin = o;  // BF16 rows of the slot's line windows
-        if (bwd) o = al(o + 3 * kLineRows * kC * 2);
+        o = al(o + 3 * kLineRows * kC * 2);
         segi = o;
         // the forward's table keeps a sample -> segment map of kMapCapF
         // samples only, which lets two forward CTAs share an SM
@@ -139,24 +141,27 @@ __device__ __forceinline__ void init_pad_columns(unsigned char* hb, int rows_per
     }
 }
 
-// Layer 0 (K = 32 over X | ones | zeros; W0's columns 24..31 are zero).
+// Layer 0 (K = 32 over X | ones | zeros, or X | zeros; W0's columns 24..31
+// are zero) of a feature buffer of COLS columns with X at column XCOL.
+template <int COLS, int XCOL>
 __device__ __forceinline__ void issue_l0(const unsigned char* sm, const Smem24& L, uint32_t hb, uint32_t d0)
 {
-    const uint32_t abase = tc::smem_addr(sm + hb + (kXCol / 8) * 128), bbase = tc::smem_addr(sm + L.w0);
+    const uint32_t abase = tc::smem_addr(sm + hb + (XCOL / 8) * 128), bbase = tc::smem_addr(sm + L.w0);
 #pragma unroll
     for (int j = 0; j < kCP / 16; ++j) {
-        const uint64_t a = tc::smem_desc(abase + j * 256, 128, (kHBCols / 8) * 128);
+        const uint64_t a = tc::smem_desc(abase + j * 256, 128, (COLS / 8) * 128);
         const uint64_t b = tc::smem_desc(bbase + j * 256, 128, (kCP / 8) * 128);
         tc::mma_bf16(d0, a, b, tc::idesc_bf16(kRows, kH, 0, 0), j > 0);
     }
 }
 
+template <int COLS>
 __device__ __forceinline__ void issue_l1(const unsigned char* sm, const Smem24& L, uint32_t hb, uint32_t d1)
 {
     const uint32_t abase = tc::smem_addr(sm + hb), bbase = tc::smem_addr(sm + L.w1);
 #pragma unroll
     for (int j = 0; j < kH / 16; ++j) {
-        const uint64_t a = tc::smem_desc(abase + j * 256, 128, (kHBCols / 8) * 128);
+        const uint64_t a = tc::smem_desc(abase + j * 256, 128, (COLS / 8) * 128);
         const uint64_t b = tc::smem_desc(bbase + j * 256, 128, (kH / 8) * 128);
         tc::mma_bf16(d1, a, b, tc::idesc_bf16(kRows, kH, 0, 0), j > 0);
     }
@@ -167,10 +172,40 @@ __device__ __forceinline__ void issue_l1(const unsigned char* sm, const Smem24& 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void half_barrier(int h) { asm volatile("bar.sync %0, 128;" ::"r"(1 + h) : "memory"); }
 
+// First row of line m's window for the slot whose leaf box (min, size) is
+// `box`: two rows below the leaf's first cell, clamped to the line.
+__device__ __forceinline__ int line_window_lo(const FusedParams& p, const float* box, int m)
+{
+    const int Ln = p.field.line_len[m];
+    if (Ln <= kLineRows) return 0;
+    // x line: the ROI-normalised x; z line: the raw z; y line: the local y
+    const float u = m == 0 ? roi_coord(box[0], p.field.roi_min[0], p.field.roi_max[0]) : (m == 2 ? box[2] : -1.0f);
+    const int lo = (int)floorf(((u + 1.0f) * 0.5f) * (float)(Ln - 1)) - 2;
+    return max(0, min(lo, Ln - kLineRows));
+}
+
+// Stages rows lo .. lo + kLineRows - 1 of each line (3 x 16 bytes per row)
+// into LW and records lo in s_lo (the item's leaf box is segment 0's).
+__device__ __forceinline__ void stage_line_windows(const FusedParams& p, const float* box, unsigned char* LW,
+                                                   int* s_lo)
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int lo = line_window_lo(p, box, m);
+        if (threadIdx.x == 0) s_lo[m] = lo;
+        const int n16 = 3 * min(kLineRows, p.field.line_len[m] - lo);
+        const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const unsigned char*>(p.field.line[m]) +
+                                                          (size_t)lo * (kC * 2));
+        uint4* dst = reinterpret_cast<uint4*>(LW + m * (kLineRows * kC * 2));
+        for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+}
+
 // VM feature of one sample, all 24 channels: planes (BF16, shared memory) and
-// lines (BF16, global), plane 2 first, corners in order.
-__device__ __forceinline__ void gather24(const FusedParams& p, const unsigned char* sm, const SampleGeo& g,
-                                         float (&f)[kC])
+// lines (BF16, the slot's window in shared memory when both taps are inside
+// it, else global), plane 2 first, corners in order.
+__device__ __forceinline__ void gather24(const FusedParams& p, const unsigned char* sm, const unsigned char* LW,
+                                         const int* s_lo, const SampleGeo& g, float (&f)[kC])
 {
 #pragma unroll
     for (int m = 2; m >= 0; --m) {
@@ -179,7 +214,12 @@ __device__ __forceinline__ void gather24(const FusedParams& p, const unsigned ch
         const Corner2 k = corners2(g.pu[m], g.pv[m], Hm, Wm);
         const Corner1 l = corners1(g.lu[m], L);
         const unsigned char* P = sm + (size_t)p.plane_off[m] * 2;
-        const unsigned char* V = reinterpret_cast<const unsigned char*>(p.field.line[m]);
+        const int r0 = l.x0 - s_lo[m], r1 = l.x1 - s_lo[m];
+        const bool inwin = (unsigned)r0 < (unsigned)kLineRows && (unsigned)r1 < (unsigned)kLineRows;
+        const unsigned char* V0 = inwin ? LW + (size_t)m * (kLineRows * kC * 2) + r0 * (kC * 2)
+                                        : reinterpret_cast<const unsigned char*>(p.field.line[m]) + l.x0 * (kC * 2);
+        const unsigned char* V1 = inwin ? LW + (size_t)m * (kLineRows * kC * 2) + r1 * (kC * 2)
+                                        : reinterpret_cast<const unsigned char*>(p.field.line[m]) + l.x1 * (kC * 2);
         float ma[kC];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -196,8 +236,8 @@ __device__ __forceinline__ void gather24(const FusedParams& p, const unsigned ch
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             float v0[8], v1[8];
-            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x0 * (kC * 2) + 16 * q)), v0);
-            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(V + l.x1 * (kC * 2) + 16 * q)), v1);
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(V0 + 16 * q), v0);
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(V1 + 16 * q), v1);
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const float ve = fmaf(v0[i], l.w0, v1[i] * l.w1);
@@ -214,6 +254,7 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
     __shared__ __align__(8) uint64_t bar_mma[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_ctl[8];
+    __shared__ int s_lo[3];
     const Smem24 L(p.plane_off[3], p.gplane_off[3], false);
     const int tid = threadIdx.x, h = tid / kRows, t = tid % kRows;
     if (tid < 32) tc::tmem_alloc(&s_tmem, kTmemF);
@@ -224,8 +265,6 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
         mbar_init(&bar_mma[1], 1);
     }
     load_weights(p, sm, L);
-    init_pad_columns(sm + L.hb[0], tid, kThreadsF);
-    init_pad_columns(sm + L.hb[1], tid, kThreadsF);
     tc::fence_smem_to_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -244,6 +283,7 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {
+            stage_line_windows(p, tab.box, sm + L.lwin, s_lo);
             if (!mbar_wait(&bar_tma, tma_phase)) {
                 set_err(p.err, ATDF_DEVERR_TREE);
                 mbar_wait(&bar_tma, tma_phase);
@@ -261,23 +301,27 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
             float w = 0.0f, ts = 0.0f;
             int si = -1;
             if (valid) {
-                const SampleState st = sample_state(p, tab, it, k);
+                const SampleState st = sample_state(p, tab, it, k, false);
                 w = st.w;
                 ts = st.t;
                 si = st.si;
                 if (real) {
                     const SampleGeo g = sample_geo_fast(p, tab, st.node, st.pos);
-                    gather24(p, sm, g, f);
+                    gather24(p, sm, sm + L.lwin, s_lo, g, f);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 3; ++q) store_bf16x8(hbh + hb_off(t, kXCol + 8 * q), f + 8 * q);
+            for (int q = 0; q < 3; ++q) store_bf16x8(hbh + hbf_off(t, 8 * q), f + 8 * q);
+            {
+                const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                store_bf16x8(hbh + hbf_off(t, kC), zero);  // K padding (the previous tile's H0 there)
+            }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
             half_barrier(h);
             if (t == 0) {
                 tc::fence_after_sync();
-                issue_l0(sm, L, L.hb[h], d0);
+                issue_l0<kHBColsF, 0>(sm, L, L.hb[h], d0);
                 tc::commit(&bar_mma[h]);
             }
             alive = wait_mma(&bar_mma[h], mma_phase, p.err);
@@ -290,15 +334,15 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
                 tc::wait_ld();
 #pragma unroll
                 for (int i = 0; i < 16; ++i) v[i] = silu(v[i] + bb[i]);
-                store_bf16x8(hbh + hb_off(t, 16 * j), v);
-                store_bf16x8(hbh + hb_off(t, 16 * j + 8), v + 8);
+                store_bf16x8(hbh + hbf_off(t, 16 * j), v);
+                store_bf16x8(hbh + hbf_off(t, 16 * j + 8), v + 8);
             }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
             half_barrier(h);
             if (t == 0) {
                 tc::fence_after_sync();
-                issue_l1(sm, L, L.hb[h], d1);
+                issue_l1<kHBColsF>(sm, L, L.hb[h], d1);
                 tc::commit(&bar_mma[h]);
             }
             alive = wait_mma(&bar_mma[h], mma_phase, p.err) && alive;
@@ -313,11 +357,24 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
 #pragma unroll
                 for (int i = 0; i < 16; ++i) z = fmaf(silu(v[i] + bb[i]), ww[i], z);
             }
-            if (valid) {
-                const float v = act_fwd(lact, z, beta) * w;
-                atomicAdd(&tab.acc[si], v);
-                if (p.bins) add_to_bins(p, tab, si, ts, v);
+            // the samples' contributions to their segments: the rows of a
+            // warp hold consecutive samples, so each segment's samples form
+            // a run of lanes; a segmented scan leaves each run's sum in its
+            // last lane, which adds it to the segment's entry
+            const float v = valid ? act_fwd(lact, z, beta) * w : 0.0f;
+            {
+                const int lane = t & 31;
+                float run = v;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const float o = __shfl_up_sync(0xffffffffu, run, off);
+                    const int ko = __shfl_up_sync(0xffffffffu, si, off);
+                    if (lane >= off && ko == si) run += o;
+                }
+                const int next = __shfl_down_sync(0xffffffffu, si, 1);
+                if (valid && (lane == 31 || next != si)) atomicAdd(&tab.acc[si], run);
             }
+            if (valid && p.bins) add_to_bins(p, tab, si, ts, v);
             tc::fence_before_sync();
             half_barrier(h);
         }
@@ -335,18 +392,6 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
 // backward: one half of 128 rows, two threads per row (group g = tid / 128)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cta_barrier() { asm volatile("bar.sync 1, 384;" ::: "memory"); }
-
-// First row of line m's window for the slot whose leaf box (min, size) is
-// `box`: two rows below the leaf's first cell, clamped to the line.
-__device__ __forceinline__ int line_window_lo(const FusedParams& p, const float* box, int m)
-{
-    const int Ln = p.field.line_len[m];
-    if (Ln <= kLineRows) return 0;
-    // x line: the ROI-normalised x; z line: the raw z; y line: the local y
-    const float u = m == 0 ? roi_coord(box[0], p.field.roi_min[0], p.field.roi_max[0]) : (m == 2 ? box[2] : -1.0f);
-    const int lo = (int)floorf(((u + 1.0f) * 0.5f) * (float)(Ln - 1)) - 2;
-    return max(0, min(lo, Ln - kLineRows));
-}
 
 // Plane (bilinear) and line (linear) values of plane / line m for the 8
 // channels of group g (channels 8g .. 8g + 7) of one sample. The line rows
@@ -395,6 +440,11 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     __shared__ int s_ctl[8];
     __shared__ int s_lo[3];
     __shared__ float s_z[2][kRows];  // partial last-layer sums [group 0 / 1][row]
+    // the next tile's sample states, computed by group 2 while groups 0 and 1
+    // run the decoder's epilogues: SampleGeo (9 values), weight, segment
+    __shared__ float s_pre[10][kRows];
+    __shared__ int s_pre_si[kRows];
+    __shared__ int s_pre_node[kRows];
     // fixed-point plane-gradient accumulation of the current slot
     __shared__ float s_tcum;    // sum of |contribution| over the slot's tiles so far
     __shared__ float s_tfirst;  // the same over its first tile (scale choice)
@@ -425,6 +475,10 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     // feature step (400 + 24 g .. + 23)
     const uint32_t d0 = tbase, d1 = tbase + 64, dacc = tbase + 128, dline = tbase + 320;
     const uint32_t stash = tbase + 256 + 12 * grp, vstash = tbase + 400 + 24 * grp;
+    // per-row sums of dz * H1 over all tiles (the last layer's weight
+    // gradient before the sum over rows): group 0 at 224..255, group 1 at
+    // 472..503
+    const uint32_t dw2 = grp == 0 ? tbase + 224 : tbase + 472;
     SegTab tab = seg_tab(reinterpret_cast<float*>(sm + L.segi));
     const float* bias = reinterpret_cast<const float*>(sm + L.bias);
     const float beta = p.mlp.softplus_beta;
@@ -439,7 +493,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     unsigned char* gb = sm + L.g;
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true, had_tile = false;
-    float gw2 = 0.f, gb2 = 0.f;  // lane owns one last-layer column of its group (groups 0, 1)
+    float gb2 = 0.f;             // group 0: this row's sum of dz over all tiles
     float scale = 0.f;           // the slot's fixed-point scale
     int ntiles = 0;              // tiles of the slot
     bool lacc = false;           // the line MMA has written the slot's accumulator
@@ -467,18 +521,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             scale = 0.f;
             ntiles = 0;
             lacc = false;
-            // the slot's line windows (the item's leaf is segment 0's): rows
-            // lo .. lo + kLineRows - 1 of each line, 3 x 16 bytes per row
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                const int lo = line_window_lo(p, tab.box, m);
-                if (tid == 0) s_lo[m] = lo;
-                const int n16 = 3 * min(kLineRows, p.field.line_len[m] - lo);
-                const uint4* src = reinterpret_cast<const uint4*>(
-                    reinterpret_cast<const unsigned char*>(p.field.line[m]) + (size_t)lo * (kC * 2));
-                uint4* dst = reinterpret_cast<uint4*>(lw + m * (kLineRows * kC * 2));
-                for (int i = tid; i < n16; i += kThreadsB) dst[i] = __ldg(src + i);
-            }
+            stage_line_windows(p, tab.box, lw, s_lo);
             if (!mbar_wait(&bar_tma, tma_phase)) {
                 set_err(p.err, ATDF_DEVERR_TREE);
                 mbar_wait(&bar_tma, tma_phase);
@@ -499,7 +542,19 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             float w = 0.0f;
             int si = -1;
             bool act = false;
-            if (valid) {
+            if (t0 > 0) {  // computed during the previous tile
+                si = s_pre_si[t];
+                w = s_pre[9][t];
+                act = real && valid;
+                if (act) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        g.pu[q] = s_pre[q][t];
+                        g.pv[q] = s_pre[3 + q][t];
+                        g.lu[q] = s_pre[6 + q][t];
+                    }
+                }
+            } else if (valid) {
                 const SampleState st = sample_state(p, tab, it, k);
                 w = st.w;
                 si = st.si;
@@ -532,7 +587,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             cta_barrier();
             if (issuer) {
                 tc::fence_after_sync();
-                issue_l0(sm, L, L.hb[0], d0);
+                issue_l0<kHBCols, kXCol>(sm, L, L.hb[0], d0);
                 tc::commit(&bar_mma);
             }
             alive = wait_mma(&bar_mma, mma_phase, p.err);
@@ -555,7 +610,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             cta_barrier();
             if (issuer) {
                 tc::fence_after_sync();
-                issue_l1(sm, L, L.hb[0], d1);
+                issue_l1<kHBCols>(sm, L, L.hb[0], d1);
                 tc::commit(&bar_mma);
             }
             alive = wait_mma(&bar_mma, mma_phase, p.err) && alive;
@@ -610,33 +665,36 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     store_bf16x8(gb + g_off(t, col0 + 16 * j), da);
                     store_bf16x8(gb + g_off(t, col0 + 16 * j + 8), da + 8);
                 }
-                // last-layer weight gradient: reduce dz * silu(a1[k]) over the
-                // warp's 32 rows, halving the value set each round
-                {
+                // last-layer weight gradient: this row's dz * H1 added to its
+                // running sums in TMEM (summed over rows at the end)
 #pragma unroll
-                    for (int kk = 0; kk < 32; ++kk) a1[kk] = dz * a1[kk];
-                    int n = 32;
-#pragma unroll
-                    for (int off = 16; off >= 1; off >>= 1) {
-                        const bool upper = (lane & off) != 0;
-                        n >>= 1;
-#pragma unroll
-                        for (int kk = 0; kk < 16; ++kk) {
-                            if (kk < n) {
-                                const float send = upper ? a1[kk] : a1[kk + n];
-                                const float keep = upper ? a1[kk + n] : a1[kk];
-                                a1[kk] = keep + __shfl_xor_sync(0xffffffffu, send, off);
-                            }
-                        }
+                for (int j = 0; j < 2; ++j) {
+                    float acc[16];
+                    if (had_tile) {
+                        tc::ld_32x32b_x16(trow(dw2, 16 * j), acc);
+                        tc::wait_ld();
                     }
-                    gw2 += a1[0];
-                    if (grp == 0) {
-                        float s = dz;
 #pragma unroll
-                        for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-                        if (lane == 0) gb2 += s;
-                    }
+                    for (int i = 0; i < 16; ++i) acc[i] = had_tile ? fmaf(dz, a1[16 * j + i], acc[i]) : dz * a1[16 * j + i];
+                    tc::st_32x32b_x16(trow(dw2, 16 * j), acc);
                 }
+                gb2 += dz;
+            } else if (t0 + kRows < it.total) {
+                // group 2, part 1: the next tile's sample states (position
+                // and leaf parked in the line-coordinate slots and s_pre_node)
+                const int k2 = t0 + kRows + t;
+                int si2 = -1;
+                float w2 = 0.0f;
+                if (k2 < it.total) {
+                    const SampleState st = sample_state(p, tab, it, k2);
+                    si2 = st.si;
+                    w2 = st.w;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) s_pre[6 + q][t] = st.pos[q];
+                    s_pre_node[t] = st.node;
+                }
+                s_pre[9][t] = w2;
+                s_pre_si[t] = si2;
             }
             tc::fence_smem_to_async();
             tc::fence_before_sync();
@@ -666,6 +724,16 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     for (int i = 0; i < 16; ++i) da[i] = gv[i] * silu_grad(av[i] + bb[i]);
                     store_bf16x8(gb + g_off(t, kH + col0 + 16 * j), da);
                     store_bf16x8(gb + g_off(t, kH + col0 + 16 * j + 8), da + 8);
+                }
+            } else if (real && t0 + kRows < it.total && s_pre_si[t] >= 0) {
+                // group 2, part 2: the next tile's plane and line coordinates
+                const float pos[3] = {s_pre[6][t], s_pre[7][t], s_pre[8][t]};
+                const SampleGeo g2 = sample_geo_fast(p, tab, s_pre_node[t], pos);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    s_pre[q][t] = g2.pu[q];
+                    s_pre[3 + q][t] = g2.pv[q];
+                    s_pre[6 + q][t] = g2.lu[q];
                 }
             }
             tc::fence_smem_to_async();
@@ -918,13 +986,37 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             }
         }
     }
-    // last layer: lane l's column within its group's 32, by the halving order
-    if (mlp) {
+    // last layer: the rows' running sums reduced over the warp's 32 rows,
+    // halving the value set each round (lane l ends with one column)
+    if (mlp && had_tile) {
+        float a[32];
+        tc::ld_32x32b_x16(trow(dw2, 0), *reinterpret_cast<float(*)[16]>(a));
+        tc::ld_32x32b_x16(trow(dw2, 16), *reinterpret_cast<float(*)[16]>(a + 16));
+        tc::wait_ld();
+        int n = 32;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            const bool upper = (lane & off) != 0;
+            n >>= 1;
+#pragma unroll
+            for (int kk = 0; kk < 16; ++kk) {
+                if (kk < n) {
+                    const float send = upper ? a[kk] : a[kk + n];
+                    const float keep = upper ? a[kk + n] : a[kk];
+                    a[kk] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+                }
+            }
+        }
         int colbits = 0;
         for (int off = 16, b = 0; off >= 1; off >>= 1, ++b)
             if (lane & off) colbits |= (32 >> (b + 1));
-        atomicAdd(&p.gmlp.weight[2][col0 + colbits], gw2);
-        if (grp == 0 && lane == 0) atomicAdd(&p.gmlp.bias[2][0], gb2);
+        atomicAdd(&p.gmlp.weight[2][col0 + colbits], a[0]);
+        if (grp == 0) {
+            float s = gb2;
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            if (lane == 0) atomicAdd(&p.gmlp.bias[2][0], s);
+        }
     }
     tc::fence_before_sync();
     __syncthreads();

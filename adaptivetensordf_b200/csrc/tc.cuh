@@ -110,27 +110,40 @@ __device__ __forceinline__ void ld_32x32b_x2(uint32_t taddr, uint32_t (&r)[2])
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
 }
 
+// TMEM stores carry no memory clobber: they touch no memory the compiler
+// tracks, so shared-memory loads may be scheduled across them; their order
+// against tcgen05.ld and tcgen05.wait::st (volatile asm) is kept.
 // Thread i of the warp stores 2 words to lane (base + i), columns col..col+1.
 __device__ __forceinline__ void st_32x32b_x2(uint32_t taddr, const uint32_t (&r)[2])
 {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};" ::"r"(taddr), "r"(r[0]), "r"(r[1])
-                 : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};" ::"r"(taddr), "r"(r[0]), "r"(r[1]));
 }
 
 // Thread i of the warp stores 4 words to lane (base + i), columns col..col+3.
 __device__ __forceinline__ void st_32x32b_x4(uint32_t taddr, const uint32_t (&r)[4])
 {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(r[0]), "r"(r[1]),
-                 "r"(r[2]), "r"(r[3])
-                 : "memory");
+                 "r"(r[2]), "r"(r[3]));
+}
+
+// Thread i of the warp stores 16 words to lane (base + i), columns col..col+15.
+__device__ __forceinline__ void st_32x32b_x16(uint32_t taddr, const float (&v)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+        "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+        "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15])));
 }
 
 // Thread i of the warp stores 8 words to lane (base + i), columns col..col+7.
 __device__ __forceinline__ void st_32x32b_x8(uint32_t taddr, const uint32_t (&r)[8])
 {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
-                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
-                 : "memory");
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]));
 }
 
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
