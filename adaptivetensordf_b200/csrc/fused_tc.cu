@@ -181,6 +181,8 @@ __device__ __forceinline__ void issue_l1(const unsigned char* sm, const TCSmem& 
 }
 
 // Forward sample features of tile row t into HB (X columns); returns validity.
+// The forward walks an item's samples in order: a warp's rows follow one ray,
+// so their plane gathers and segment-table reads share addresses.
 __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned char* sm, const TCSmem& L,
                                               const SegTab& tab, const ItemInfo& it, bool real, int h, int k,
                                               int t, float& w, int& si, SampleGeo& g, float& ts)
@@ -193,7 +195,7 @@ __device__ __forceinline__ bool tile_features(const FusedParams& p, unsigned cha
     ts = 0.0f;
     si = -1;
     if (valid) {
-        const SampleState st = sample_state(p, tab, it, k);
+        const SampleState st = sample_state(p, tab, it, k, false);
         w = st.w;
         ts = st.t;
         si = st.si;
@@ -302,11 +304,22 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
 #pragma unroll
                 for (int i = 0; i < 16; ++i) z = fmaf(silu(v[i] + bb[i]), ww[i], z);
             }
-            if (valid) {
-                const float v = act_fwd(lact, z, beta) * w;
-                atomicAdd(&tab.acc[si], v);
-                if (p.bins) add_to_bins(p, tab, si, ts, v);
+            // each segment's run of lanes summed by a segmented warp scan,
+            // its last lane adding the run to the segment's entry
+            const float v = valid ? act_fwd(lact, z, beta) * w : 0.0f;
+            {
+                const int lane = t & 31;
+                float run = v;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const float o = __shfl_up_sync(0xffffffffu, run, off);
+                    const int ko = __shfl_up_sync(0xffffffffu, si, off);
+                    if (lane >= off && ko == si) run += o;
+                }
+                const int next = __shfl_down_sync(0xffffffffu, si, 1);
+                if (valid && (lane == 31 || next != si)) atomicAdd(&tab.acc[si], run);
             }
+            if (valid && p.bins) add_to_bins(p, tab, si, ts, v);
             tc::fence_before_sync();
             half_barrier(h);
         }

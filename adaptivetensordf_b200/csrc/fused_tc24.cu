@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     }
                 }
             } else if (valid) {
-                const SampleState st = sample_state(p, tab, it, k);
+                const SampleState st = sample_state(p, tab, it, k, false);
                 w = st.w;
                 si = st.si;
                 if (real) {
@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                 int si2 = -1;
                 float w2 = 0.0f;
                 if (k2 < it.total) {
-                    const SampleState st = sample_state(p, tab, it, k2);
+                    const SampleState st = sample_state(p, tab, it, k2, false);
                     si2 = st.si;
                     w2 = st.w;
 #pragma unroll
@@ -872,17 +872,32 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                 lacc = true;
                 // scatter, phase 2: the group's 8 channels to the four
                 // corners, as fixed-point integers (shared-memory integer
-                // atomics run several times faster than FP32 ones); the lane's
-                // corner order is rotated so a warp's atomics spread over
-                // texels. Channels go in a fixed order, which keeps the 24
-                // contributions in registers.
+                // atomics run several times faster than FP32 ones). A warp's
+                // rows are consecutive samples of a ray, several in one cell:
+                // lane l takes the corners from (l mod 4) on and the channels
+                // from (l / 4 mod 8) on, so up to 32 lanes in one cell add to
+                // 32 different words at each step.
                 if (valid) {
+                    const int crot = (lane >> 2) & 7;
 #pragma unroll
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
                         const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
                         if (to_smem) {
-                            int* GP = gpl + gpo[m];
+                            // gr[i] = gv[m][(i + crot) mod 8] (a three-stage rotation)
+                            float gr[8];
+#pragma unroll
+                            for (int i = 0; i < 8; ++i) gr[i] = gv[m][i];
+#pragma unroll
+                            for (int b = 0; b < 3; ++b) {
+                                const bool on = (crot >> b) & 1;
+                                float nx[8];
+#pragma unroll
+                                for (int i = 0; i < 8; ++i) nx[i] = on ? gr[(i + (1 << b)) & 7] : gr[i];
+#pragma unroll
+                                for (int i = 0; i < 8; ++i) gr[i] = nx[i];
+                            }
+                            int* GP = gpl + gpo[m] + 8 * grp;
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
                                 float wj;
@@ -890,7 +905,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                                 const float ws = wj * scale;
 #pragma unroll
                                 for (int i = 0; i < 8; ++i)
-                                    atomicAdd(&GP[tx + 8 * grp + i], __float2int_rn(ws * gv[m][i]));
+                                    atomicAdd(&GP[tx + ((i + crot) & 7)], __float2int_rn(ws * gr[i]));
                             }
                         } else {
                             float* GG = p.gfield.plane[m] + it.slot * (int64_t)(Hm * Wm * kC);
