@@ -114,6 +114,49 @@ __global__ void item_count_kernel(Ws w)
     }
 }
 
+// The item queue of the forwards: for each slot in the slot queue's order
+// (slot_cursor) its items (slot, 0 .. n - 1), at the exclusive prefix of the
+// item counts in that order; counters[4] = the number of items. One block.
+__global__ void item_queue_kernel(Ws w)
+{
+    __shared__ int warp_sum[32];
+    __shared__ int s_base;
+    const int n = (int)w.nslot + 1;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+        const int q = c0 + threadIdx.x;
+        int sl = -1, ni = 0;
+        if (q < n) {
+            sl = w.slot_cursor[q];
+            ni = w.item_offset[sl + 1] - w.item_offset[sl];
+        }
+        int incl = ni;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int x = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += x;
+        }
+        if (lane == 31) warp_sum[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int v = lane < nw ? warp_sum[lane] : 0;
+            for (int off = 1; off < 32; off <<= 1) {
+                const int x = __shfl_up_sync(0xffffffffu, v, off);
+                if (lane >= off) v += x;
+            }
+            if (lane < nw) warp_sum[lane] = v;  // inclusive over warps
+        }
+        __syncthreads();
+        const int pos = s_base + (wid > 0 ? warp_sum[wid - 1] : 0) + incl - ni;
+        for (int i = 0; i < ni; ++i) w.item_queue[pos + i] = make_int2(sl, i);
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += warp_sum[nw - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) w.counters[4] = s_base;
+}
+
 // Zeroes the plane gradients of the slots that no segment touches; the
 // tensor-core backward writes every touched slot's gradient itself.
 __global__ void zero_untouched_slots_kernel(Ws w, atdf_field_grad_t g, atdf_field_t f)
@@ -979,6 +1022,10 @@ static int project_forward(const atdf_tree_t* tree, const atdf_field_t* field, c
     ATDF_LAUNCH_CHECK();
     scan_exclusive_i32_kernel<<<1, 1024, 0, s>>>(w.item_offset, w.nslot + 2, nullptr);
     ATDF_LAUNCH_CHECK();
+    if (!var) {  // the tensor-core forwards take work by item
+        item_queue_kernel<<<1, 1024, 0, s>>>(w);
+        ATDF_LAUNCH_CHECK();
+    }
     st = var ? launch_persistent(var->fwd, var->smem(p.plane_off[3], false), p, s) : launch_tc_forward(p, s);
     if (st != ATDF_OK) return st;
     if (num_rays > 0) {

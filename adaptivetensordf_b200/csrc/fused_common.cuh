@@ -34,7 +34,8 @@ struct Ws {
     int32_t* slot_offset;  // [nslot + 2]
     int32_t* slot_cursor;  // [nslot + 1]: bucket cursors, then the queue's slot order
     int32_t* item_offset;  // [nslot + 2]
-    int32_t* counters;     // [8]
+    int32_t* counters;     // [8]: the queues' positions (0, 1), the item queue's length (4)
+    int2* item_queue;      // (slot, item of the slot) in the slot queue's order
     int64_t cap;
     int64_t nslot;
 };
@@ -74,6 +75,7 @@ static size_t ws_layout(int64_t R, int max_depth, int64_t nslot, char* base, Ws*
     x.slot_cursor = (int32_t*)carve(p, (nslot + 1) * 4);
     x.item_offset = (int32_t*)carve(p, (nslot + 2) * 4);
     x.counters = (int32_t*)carve(p, 8 * 4);
+    x.item_queue = (int2*)carve(p, (nslot + 3 + cap / kSegItem) * 8);
     x.cap = cap;
     x.nslot = nslot;
     if (w) *w = x;
@@ -228,11 +230,15 @@ __device__ __forceinline__ SegTab seg_tab(float* base)
 // when the item starts a new slot. Returns the item's slot, or -1 when the
 // queue is empty. Items of up to map_cap (<= kSegMapCap) samples get the
 // sample -> segment byte map, larger ones a binary search.
-// A work item's samples are visited in the order k -> k * 104729 mod total
-// (a permutation: the prime exceeds any item's sample count). Consecutive
-// samples, which share a warp, then come from different rays and depths in
-// the leaf and touch different texels, so their shared-memory atomics do not
-// collide the way the samples along one ray would.
+// sample_state(permute = true) visits a work item's samples in the order
+// k -> k * 104729 mod total (a permutation: the prime exceeds any item's
+// sample count). Consecutive samples, which share a warp, then come from
+// different rays and depths in the leaf and touch different texels, so their
+// shared-memory atomics do not collide the way the samples along one ray
+// would. The FP32 kernels and the 16-channel tensor-core backward use it; the
+// tensor-core forwards and the 24-channel backward visit samples in order
+// (gathers along a ray share texels; that backward rotates its atomics
+// instead).
 constexpr int kSamplePermPrime = 104729;
 
 struct ItemInfo {
@@ -276,13 +282,48 @@ __device__ __forceinline__ void init_item_queue(int* s_ctl)
     s_ctl[7] = 0;
 }
 
+// by_item (the forwards, which keep no per-slot state between items): work
+// is handed out by item from the item queue (the slot queue's order, each
+// slot's items in a row), so the items of a large slot spread over several
+// CTAs; a CTA stages a slot's planes when its next item is of another slot.
 __device__ __forceinline__ ItemInfo next_item(const FusedParams& p, int queue, float* sm, SegTab tab, uint64_t* bar,
-                                              int* s_ctl, bool want_dI, int map_cap = kSegMapCap)
+                                              int* s_ctl, bool want_dI, int map_cap = kSegMapCap,
+                                              bool by_item = false)
 {
     const Ws& w = p.ws;
     const int tid = threadIdx.x;
     if (tid < 32) {
-        if (tid == 0) {
+        if (tid == 0 && by_item) {
+            int slot = -1, b0 = 0, nseg = 0, flags = 0;
+            const int q = atomicAdd(&w.counters[queue], 1);
+            if (q < w.counters[4]) {
+                const int2 e = w.item_queue[q];
+                slot = e.x;
+                const int nit = w.item_offset[slot + 1] - w.item_offset[slot];
+                if (slot != s_ctl[4]) {
+                    s_ctl[4] = slot;
+                    flags |= 1;
+                    if (slot < w.nslot) {
+                        const int esz = p.field.dtype == ATDF_BF16 ? 2 : 4;
+                        uint32_t bytes = 0;
+                        for (int m = 0; m < 3; ++m)
+                            bytes += (uint32_t)(p.field.plane_h[m] * p.field.plane_w[m] * p.field.channels * esz);
+                        mbar_expect_tx(bar, bytes);
+                        flags |= 4;
+                    }
+                }
+                const int cnt = w.slot_offset[slot + 1] - w.slot_offset[slot];
+                const int per = (cnt + nit - 1) / nit;
+                b0 = w.slot_offset[slot] + e.y * per;
+                nseg = min(b0 + per, w.slot_offset[slot + 1]) - b0;
+                if (e.y == nit - 1) flags |= 2;
+                s_ctl[7] = nit;
+            }
+            s_ctl[0] = slot;
+            s_ctl[1] = b0;
+            s_ctl[2] = nseg;
+            s_ctl[3] = flags;
+        } else if (tid == 0) {
             int slot = -1, b0 = 0, nseg = 0, flags = 0;
             if (s_ctl[5] >= s_ctl[6]) {  // the current slot is done: take the next one with work
                 const int nslots = (int)w.nslot + 1;  // plane slots + the out-of-ROI bucket

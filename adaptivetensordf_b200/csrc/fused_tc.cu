@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kThreadsTC, 2) tc_forward_kernel(FusedParams p
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true;
     while (alive) {
-        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false);
+        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false, kSegMapCap, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {

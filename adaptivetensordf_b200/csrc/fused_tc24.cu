@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kThreadsF, 2) tc24_forward_kernel(FusedParams 
     uint32_t tma_phase = 0, mma_phase = 0;
     bool alive = true;
     while (alive) {
-        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false, kMapCapF);
+        const ItemInfo it = next_item(p, 0, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, false, kMapCapF, true);
         if (it.slot < 0) break;
         const bool real = it.slot < p.ws.nslot;
         if (real && it.first) {
