@@ -404,7 +404,7 @@ __device__ __forceinline__ bool tile_features_half(const FusedParams& p, unsigne
     w = 0.0f;
     si = -1;
     if (valid) {
-        const SampleState st = sample_state(p, tab, it, k);
+        const SampleState st = sample_state(p, tab, it, k, false);
         w = st.w;
         si = st.si;
         if (real) {

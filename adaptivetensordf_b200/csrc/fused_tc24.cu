@@ -497,6 +497,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
     float scale = 0.f;           // the slot's fixed-point scale
     int ntiles = 0;              // tiles of the slot
     bool lacc = false;           // the line MMA has written the slot's accumulator
+    bool gzero = false;          // the slot's global gradient has been zeroed (its first FP32 tile)
     while (alive) {
         const ItemInfo it = next_item(p, 1, reinterpret_cast<float*>(sm), tab, &bar_tma, s_ctl, true);
         if (it.slot < 0) break;
@@ -504,14 +505,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
         if (real && it.first) {
             for (int i = tid * 4; i < gpl_words; i += kThreadsB * 4)
                 *reinterpret_cast<int4*>(gpl + i) = make_int4(0, 0, 0, 0);
-            // the slot's global gradient starts at zero (the caller does not
-            // clear it): a tile that overflows the fixed-point range adds to it
-            for (int m = 0; m < 3; ++m) {
-                const int pf = p.field.plane_h[m] * p.field.plane_w[m] * kC;
-                float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
-                for (int i = tid * 4; i < pf; i += kThreadsB * 4)
-                    *reinterpret_cast<float4*>(dst + i) = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            gzero = false;
             if (tid == 0) {
                 s_tcum = 0.f;
                 s_tfirst = 0.f;
@@ -856,6 +850,19 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                 const bool to_smem =
                     s_tcum * scale + (float)ntiles * (0.5f * kRows * 3 * 4 * kC) <= 1073741824.0f;
                 if (!to_smem && issuer) s_fb = 1;
+                if (!to_smem && !gzero) {
+                    // the slot's first tile in FP32 (the same decision in every
+                    // thread): its global gradient starts at zero (the caller
+                    // does not clear it), then tiles and the flush add to it
+                    for (int m = 0; m < 3; ++m) {
+                        const int pf = p.field.plane_h[m] * p.field.plane_w[m] * kC;
+                        float* dst = p.gfield.plane[m] + it.slot * (int64_t)pf;
+                        for (int i = tid * 4; i < pf; i += kThreadsB * 4)
+                            *reinterpret_cast<float4*>(dst + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                    __syncthreads();
+                    gzero = true;
+                }
                 if (issuer) {  // line gradients of the tile into the slot's accumulator (overlaps the atomics)
                     tc::fence_after_sync();
                     const uint32_t abase = tc::smem_addr(gb), bbase = tc::smem_addr(hb);

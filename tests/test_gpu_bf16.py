@@ -67,18 +67,21 @@ def test_bf16_tensor_core_projection(oracle, depth, R, M, seed_j):
         assert v < BF16_TOL, k
 
 
-def test_bf16_plane_gradient_dynamic_range(oracle):
+@pytest.mark.parametrize("C", [16, 24])
+def test_bf16_plane_gradient_dynamic_range(oracle, C):
     """The tensor-core backward sums each leaf's plane gradients as fixed-point
     integers with a per-leaf scale chosen from the first tiles, and sends a
-    tile that would exceed the integer range to global memory in FP32. Image
-    gradients spread over twelve decades (random signs) make the tiles of a
-    leaf differ by orders of magnitude, so both paths run; every leaf's plane
-    gradient must still match the oracle to BF16_TOL of its own norm."""
+    tile that would exceed the integer range to global memory in FP32 (the
+    24-channel kernel zeroes a leaf's global gradient at its first such
+    tile). Image gradients spread over twelve decades (random signs) make the
+    tiles of a leaf differ by orders of magnitude, so both paths run; every
+    leaf's plane gradient must still match the oracle to BF16_TOL of its own
+    norm."""
     import adaptivetensordf_b200 as ab
 
     depth, R, M, seed_j = 3, 900, 12, 3
     L = (17 - 1) * (1 << depth)
-    tree, geo, o, d = gpu_scene(depth, 16, 17, (L, 17, L), [64, 64], R, seed=41)
+    tree, geo, o, d = gpu_scene(depth, C, 17, (L, 17, L), [64, 64], R, seed=41)
     geo.precision = "bf16"
     geo.RefreshLowPrecision()
     td, fd, md = oracle_views(tree, geo)
