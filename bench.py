@@ -738,11 +738,13 @@ def run_ours(args, rank, world):
     # gradient writes still in L2 when the kernel ends are not counted there
     roof2["traffic"] = 129719040 + 179244288 if R == 16384 else None
     roof2["traffic_source"] = "profiles/tc_backward_dram_c2_16384rays.md" if R == 16384 else None
-    roof5["traffic"] = None
-    # this library's kernels per uniform training step of the BF16 form: 13 for
-    # sampling, bucketing (with the slot order), projection and loss, and one
-    # Adam launch for the 12 parameters
-    launches_per_step = 15
+    # the same for the C5 rank-24 backward (full-size capture, 3 launches)
+    roof5["traffic"] = 177041835 + 283314176 if R == 16384 else None
+    roof5["traffic_source"] = "profiles/launches_c5_bf16_16384rays.md" if R == 16384 else None
+    # this library's kernels per uniform training step of the BF16 form: 12
+    # for sampling, bucketing (slot order, item queue) and the forward, the
+    # loss, 2 for the backward and one Adam launch for the 12 parameters
+    launches_per_step = 16
     h2d = sum(t.numel() * t.element_size() for t in make_host_shapes(R))
     line = {
         "metric": METRIC,
