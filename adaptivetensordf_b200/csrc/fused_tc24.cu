@@ -884,45 +884,51 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                 // lane l takes the corners from (l mod 4) on and the channels
                 // from (l / 4 mod 8) on, so up to 32 lanes in one cell add to
                 // 32 different words at each step.
-                if (valid) {
+                if (valid && to_smem) {
                     const int crot = (lane >> 2) & 7;
 #pragma unroll
                     for (int m = 0; m < 3; ++m) {
                         const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
                         const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
-                        if (to_smem) {
-                            // gr[i] = gv[m][(i + crot) mod 8] (a three-stage rotation)
-                            float gr[8];
+                        // gr[i] = gv[m][(i + crot) mod 8] (a three-stage rotation)
+                        float gr[8];
 #pragma unroll
-                            for (int i = 0; i < 8; ++i) gr[i] = gv[m][i];
+                        for (int i = 0; i < 8; ++i) gr[i] = gv[m][i];
 #pragma unroll
-                            for (int b = 0; b < 3; ++b) {
-                                const bool on = (crot >> b) & 1;
-                                float nx[8];
+                        for (int b = 0; b < 3; ++b) {
+                            const bool on = (crot >> b) & 1;
+                            float nx[8];
 #pragma unroll
-                                for (int i = 0; i < 8; ++i) nx[i] = on ? gr[(i + (1 << b)) & 7] : gr[i];
+                            for (int i = 0; i < 8; ++i) nx[i] = on ? gr[(i + (1 << b)) & 7] : gr[i];
 #pragma unroll
-                                for (int i = 0; i < 8; ++i) gr[i] = nx[i];
-                            }
-                            int* GP = gpl + gpo[m] + 8 * grp;
+                            for (int i = 0; i < 8; ++i) gr[i] = nx[i];
+                        }
+                        int* GP = gpl + gpo[m] + 8 * grp;
 #pragma unroll
-                            for (int j = 0; j < 4; ++j) {
-                                float wj;
-                                const int tx = corner_texel(kc, (j + lane) & 3, Wm, wj) * kGP;
-                                const float ws = wj * scale;
+                        for (int j = 0; j < 4; ++j) {
+                            float wj;
+                            const int tx = corner_texel(kc, (j + lane) & 3, Wm, wj) * kGP;
+                            const float ws = wj * scale;
 #pragma unroll
-                                for (int i = 0; i < 8; ++i)
-                                    atomicAdd(&GP[tx + ((i + crot) & 7)], __float2int_rn(ws * gr[i]));
-                            }
-                        } else {
-                            float* GG = p.gfield.plane[m] + it.slot * (int64_t)(Hm * Wm * kC);
+                            for (int i = 0; i < 8; ++i)
+                                atomicAdd(&GP[tx + ((i + crot) & 7)], __float2int_rn(ws * gr[i]));
+                        }
+                    }
+                }
+                // a tile beyond the fixed-point range: FP32 atomics to the
+                // slot's global gradient (rare; kept out of the unrolled code)
+                if (valid && !to_smem) {
 #pragma unroll
-                            for (int j = 0; j < 4; ++j) {
-                                float wj;
-                                const int tx = corner_texel(kc, j, Wm, wj) * kC;
+                    for (int m = 0; m < 3; ++m) {
+                        const int Hm = p.field.plane_h[m], Wm = p.field.plane_w[m];
+                        const Corner2 kc = corners2(g.pu[m], g.pv[m], Hm, Wm);
+                        float* GG = p.gfield.plane[m] + it.slot * (int64_t)(Hm * Wm * kC);
+#pragma unroll 1
+                        for (int j = 0; j < 4; ++j) {
+                            float wj;
+                            const int tx = corner_texel(kc, j, Wm, wj) * kC;
 #pragma unroll
-                                for (int i = 0; i < 8; ++i) atomicAdd(&GG[tx + 8 * grp + i], wj * gv[m][i]);
-                            }
+                            for (int i = 0; i < 8; ++i) atomicAdd(&GG[tx + 8 * grp + i], wj * gv[m][i]);
                         }
                     }
                 }
