@@ -352,6 +352,76 @@ def proposal_gate(tree, cfg, dev_batches, budget, steps=400):
     return res
 
 
+def projection_psnr_race(tree, cfg, target_db=49.0, steps=3000, nb=48, budget=64, every=100):
+    """Wall time of the BF16 form to a held-out projection PSNR on the
+    workload, with the uniform sampler and through the learned proposal
+    (`budget` samples per ray, judge every 10th step): both train from the
+    same seeded initialisation on the same `nb` batches; every `every` steps
+    the uniform projection of a held-out batch of 16384 rays is compared
+    with its analytic targets (10 log10(peak^2 / MSE), peak = the batch's
+    largest target), outside the clock. The projection domain stands in for
+    the volume PSNR here: voxelising the 1024 x 1024 x 256 slab of 5000
+    ellipsoids for a volume reference would cost more than the whole run."""
+    import torch
+
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+    from adaptivetensordf_b200.optim import Adam
+    from adaptivetensordf_b200.proposal import ProposalSchedule
+
+    R = cfg.rays_per_batch
+    batches = [tuple(torch.from_numpy(a).cuda() for a in b) for b in make_batches(cfg, R, nb, 7000, device="cuda")]
+    vo, vd, vy = (torch.from_numpy(a).cuda() for a in make_batches(cfg, R, 1, 9999, device="cuda")[0])
+    peak = float(vy.max())
+    M = cfg.max_samples_per_node
+
+    def run(with_prop):
+        geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003, init_scale=0.05)
+        geo.precision = "bf16"
+        geo.RefreshLowPrecision()
+        opt = Adam([{"params": list(geo.planes) + list(geo.lines), "lr": 0.01},
+                    {"params": list(geo.decoder_weight) + list(geo.decoder_bias), "lr": 5e-4}], geometry=geo)
+        prop = ProposalSchedule(tree, geo, M, budget=budget) if with_prop else None
+        clock, reached, best, curve = 0.0, None, -1.0, []
+        torch.cuda.synchronize()
+        for k in range(steps):
+            t1 = time.perf_counter()
+            o, d, y = batches[k % nb]
+            rays = ab.RayList(o, d)
+            img = prop.project(rays, 1 + k, y) if prop else geo.ProjectRays(tree, rays, M, 1 + k)
+            loss, gimg = ab.MseLossAndGrad(img, y, 1.0)
+            img.backward(gimg)
+            opt.step()
+            opt.zero_grad(set_to_none=True)
+            if (k + 1) % every:
+                clock += time.perf_counter() - t1
+                continue
+            torch.cuda.synchronize()
+            clock += time.perf_counter() - t1
+            with torch.no_grad():
+                v = geo.ProjectRays(tree, ab.RayList(vo, vd), M, 0).reshape(-1)
+                db = 10.0 * math.log10(peak * peak / float(((v - vy) ** 2).mean()))
+            best = max(best, db)
+            curve.append([k + 1, round(clock, 3), round(db, 3)])
+            if db >= target_db:
+                reached = clock
+                break
+        geo.CheckErrors()
+        out = {"seconds": reached, "steps": curve[-1][0], "best_db": best, "curve": curve[::5]}
+        if prop:
+            out.update({k: v for k, v in prop.stats().items() if k in ("judge_steps", "proposal_steps",
+                                                                         "uniform_steps", "proposal_error")})
+        return out
+
+    res = {"target_db": target_db, "metric": "held-out projection PSNR (16384 rays, analytic targets)",
+           "workload": cfg.name, "budget_per_ray": budget, "bf16": run(False), "bf16+prop": run(True)}
+    if res["bf16"]["seconds"] and res["bf16+prop"]["seconds"]:
+        res["ratio_bf16_over_bf16+prop"] = res["bf16"]["seconds"] / res["bf16+prop"]["seconds"]
+    del batches
+    torch.cuda.empty_cache()
+    return res
+
+
 def time_entry_points(tree, geo, o, d, M, seed, reps=10):
     """GPU time of the fused forward and backward entry points alone, called
     through the C ABI with preallocated gradients and the forward's
@@ -686,6 +756,7 @@ def run_ours(args, rank, world):
     prop5 = measure_proposal(args, tree, cfg, dev, len(dev), stream, 64) if world == 1 else None
     if prop5 is not None and not args.no_gate:
         prop5["gate_run"] = proposal_gate(tree, cfg, dev, 64)
+    race5 = projection_psnr_race(tree, cfg) if (world == 1 and not args.no_psnr) else None
     del tree, dev, host
 
     # the depth-4 / rank-16 workload: plain FP32 against the chosen form
@@ -794,6 +865,8 @@ def run_ours(args, rank, world):
         line["seconds_to_psnr"] = psnr
     if psnr30:
         line["seconds_to_30db"] = psnr30
+    if race5:
+        line["proposal_form"]["seconds_to_projection_psnr"] = race5
     if not args.no_cpu_baseline:
         t = oracle_tree(cfg)
         line["cpu_baseline"] = cpu_baseline(cfg, t, args.cpu_rays, 3)
