@@ -57,8 +57,10 @@ constexpr int kGCols = 128;      // dA1 (64) | dA0 (64)
 // gradients it accumulates (in TMEM, by the line MMA). A leaf of depth d spans
 // 256 / 2^d cells of a 256-entry line, so 42 rows cover depth-3 leaves (32
 // cells, both taps and a rounding margin); samples outside the window read
-// and add to global memory.
-constexpr int kLineRows = 42;    // 3 x 42 = 126 <= 128 rows of the line MMA
+// and add to global memory. Line m's taps are columns 40 m .. 40 m + 39 of the
+// line MMA's A operand: five 16-byte groups, which thread group m zeroes and
+// fills for its row.
+constexpr int kLineRows = 40;    // 3 x 40 = 120 <= 128 rows of the line MMA
 constexpr int kLineN = 80;       // N of the line-gradient MMA (3 * 24 = 72, padded)
 constexpr int kThreadsF = 256;   // forward: two halves of 128 rows, one thread per row
 constexpr int kThreadsB = 384;   // backward: one half of 128 rows, three threads per row
@@ -640,8 +642,10 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                     }
                 }
                 s_z[grp][t] = zp;
+                // the two partial sums of a row meet within its quarter of
+                // the rows (warps q and q + 4); group 2 goes on without them
+                asm volatile("bar.sync %0, 64;" ::"r"(2 + ((tid >> 5) & 3)) : "memory");
             }
-            cta_barrier();
             if (mlp) {
                 const float z = s_z[0][t] + s_z[1][t] + bias[3 * kH];
                 const float dz = dIw * act_grad(lact, z, beta);
@@ -768,10 +772,11 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
             tc::wait_ld();
             float gv[3][8];
             if (real) {
-                if (grp == 0) {
+                {
                     const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
-                    for (int q = 0; q < kGCols / 8; ++q) *reinterpret_cast<uint4*>(gb + g_off(t, 8 * q)) = z4;
+                    for (int q = 0; q < kLineRows / 8; ++q)
+                        *reinterpret_cast<uint4*>(gb + g_off(t, kLineRows * grp + 8 * q)) = z4;
                 }
                 float tsum = 0.f;  // sum of |dX * line value| of this thread's 24 values
 #pragma unroll
@@ -799,7 +804,7 @@ __global__ void __launch_bounds__(kThreadsB, 1) tc24_backward_kernel(FusedParams
                         const int lo = s_lo[m];
                         const int i0 = l.x0 - lo, i1 = l.x1 - lo;
                         if (i0 >= 0 && i0 < kLineRows && i1 >= 0 && i1 < kLineRows) {
-                            if (grp == 0) {
+                            if (grp == m) {
                                 if (i0 == i1) {
                                     *reinterpret_cast<__nv_bfloat16*>(gb + g_off(t, m * kLineRows + i0)) =
                                         __float2bfloat16_rn(l.w0 + l.w1);
