@@ -614,7 +614,9 @@ __global__ void __launch_bounds__(kThreadsB2, 1) tc_backward2_kernel(FusedParams
                 }
             }
             s_z[h][grp][t] = zp;
-            half_barrier2(h);
+            // a row's two partial sums meet within its quarter of the half's
+            // rows (warps 8 h + q and 8 h + 4 + q)
+            asm volatile("bar.sync %0, 64;" ::"r"(4 + 4 * h + ((tid >> 5) & 3)) : "memory");
             const float z = s_z[h][0][t] + s_z[h][1][t] + bias[3 * kH];
             const float dz = dIw * act_grad(lact, z, beta);
             // dA1 = dz w2 silu'(A1) into G columns col0..col0+31
