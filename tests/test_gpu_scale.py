@@ -181,3 +181,57 @@ def test_bench_shapes_bf16_dense_window(oracle, c2_model, M):
     for k, v in errs.items():
         assert v < BF16_TOL[k.rstrip("0123456789")], k
     geo.CheckErrors()
+
+
+def test_c5_rank24_dense_window_bf16(oracle):
+    """The rank-24 kernels at the C5 headline's shapes where they split work
+    the most: 1536 rays of the C5 series through a 32 x 32-pixel window at the
+    detector's centre cross the same central leaves, so a leaf's segments fill
+    many work items (the forwards spread them over CTAs through the item
+    queue; the backward walks them in one CTA), items exceed the forward's
+    2048-sample map, and depth-3 leaves use the 40-row line windows. BF16
+    projection and gradients against the FP64 oracle on the BF16-rounded
+    parameters, with the tolerances above."""
+    import adaptivetensordf_b200 as ab
+    from adaptivetensordf_b200 import synthetic as syn
+
+    cfg = syn.CONFIGS["C5"]
+    tree = syn.adaptive_tree(cfg, syn.config_phantom(cfg, 1001), device="cuda")
+    geo = syn.make_geometry(tree, cfg.channels, cfg.grid, cfg.lines(), cfg.hidden, seed=1003)
+    geo.precision = "bf16"
+    geo.RefreshLowPrecision()
+    R, M, seed_j, w = 1536, cfg.max_samples_per_node, 61, 32
+    rng = np.random.default_rng(77)
+    img = rng.integers(0, cfg.angles, R)
+    c0 = cfg.detector // 2 - w // 2
+    px = c0 + rng.integers(0, w, R)
+    py = c0 + rng.integers(0, w, R)
+    o, d = syn.parallel_beam_rays(syn.tilt_angles(cfg), cfg.detector, img, py * cfg.detector + px, cfg.off_axis_deg)
+    td, fd, md = syn.tree_dict(tree), syn.field_dict(geo, tree), syn.mlp_dict(geo)
+    fd_b = {**fd, "planes": [_bf16(p) for p in fd["planes"]], "lines": [_bf16(x) for x in fd["lines"]]}
+    md_b = {**md, "layers": [(_bf16(wt), b.astype(np.float64)) for wt, b in md["layers"]]}
+    md_b["layers"][-1] = (md["layers"][-1][0].astype(np.float64), md["layers"][-1][1].astype(np.float64))
+    segs, so = _oracle_samples(oracle, td, o, d, M, seed_j)
+    per_leaf = np.bincount(segs["node"])
+    samples = np.bincount(segs["node"], weights=segs["n"])
+    depth = tree.node_depth.cpu().numpy()
+    print(f"\n{len(segs['n'])} segments, {int(segs['n'].sum())} samples; max segments per leaf {per_leaf.max()}, "
+          f"max samples per leaf {int(samples.max())}, depth-3 leaves hit {int((per_leaf[depth[:len(per_leaf)] == 3] > 0).sum())}")
+    assert per_leaf.max() > 3 * 128  # a leaf of several work items
+    assert samples.max() > 2 * 2048
+    out = geo.ProjectRays(tree, ab.RayList(torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()), M, seed_j)
+    ref = oracle.project_forward(fd_b, md_b, td, so, R, np.float64)
+    errs = {"image": rel_err(out.detach().cpu().numpy(), ref)}
+    gi = np.random.default_rng(11).normal(size=ref.shape)
+    out.backward(torch.from_numpy(gi.astype(np.float32)).cuda())
+    gr = oracle.project_backward(fd_b, md_b, td, so, R, gi, np.float64)
+    for m in range(3):
+        errs[f"plane{m}"] = rel_err(geo.planes[m].grad.cpu().numpy(), gr["planes"][m])
+        errs[f"line{m}"] = rel_err(geo.lines[m].grad.cpu().numpy(), gr["lines"][m])
+    for li in range(3):
+        errs[f"W{li}"] = rel_err(geo.decoder_weight[li].grad.cpu().numpy(), gr["W"][li])
+        errs[f"b{li}"] = rel_err(geo.decoder_bias[li].grad.cpu().numpy(), gr["b"][li])
+    print("rank-24 BF16 at C5's shapes: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+    for k, v in errs.items():
+        assert v < BF16_TOL[k.rstrip("0123456789")], k
+    geo.CheckErrors()
