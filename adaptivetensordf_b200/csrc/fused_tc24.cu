@@ -55,7 +55,7 @@ constexpr int kGCols = 128;      // dA1 (64) | dA0 (64)
 // The backward keeps a window of kLineRows rows of each line per slot: the
 // rows of the line values it reads (staged in shared memory) and of the line
 // gradients it accumulates (in TMEM, by the line MMA). A leaf of depth d spans
-// 256 / 2^d cells of a 256-entry line, so 42 rows cover depth-3 leaves (32
+// 256 / 2^d cells of a 256-entry line, so 40 rows cover depth-3 leaves (32
 // cells, both taps and a rounding margin); samples outside the window read
 // and add to global memory. Line m's taps are columns 40 m .. 40 m + 39 of the
 // line MMA's A operand: five 16-byte groups, which thread group m zeroes and
