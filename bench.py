@@ -867,7 +867,7 @@ def run_ours(args, rank, world):
         line["seconds_to_30db"] = psnr30
     if race5:
         line["proposal_form"]["seconds_to_projection_psnr"] = race5
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the CPU baseline and the checker run at N = 1 only
         t = oracle_tree(cfg)
         line["cpu_baseline"] = cpu_baseline(cfg, t, args.cpu_rays, 3)
         # the FP64 oracle as the checker of the BF16 form's error (C3 asks
